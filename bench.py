@@ -1,0 +1,361 @@
+#!/usr/bin/env python
+"""Benchmark of the Heston/Bates CF pricing path on B200.
+
+One step = one pass of the hot path over one batch: the 1,048,576-contract
+Bates deep-wing batch (4096 surfaces x 256 contracts, tol 1e-10) priced by
+the persistent multi-surface kernel.  Prints ONE JSON line (rank 0).
+
+  value      contracts/s, inputs resident in HBM, CUDA events on the launch
+             stream; L2 flushed (512 MiB write) before every step.
+  e2e        same metric through the public host API (pinned host buffers,
+             H2D of the step's contracts/params/offsets and D2H of prices
+             inside the timed region, wall clock around the synchronous call).
+  plain      the reference-shaped drop-in: one batch_bates call per surface
+             (host buffers, synchronous), on a sample of surfaces.
+  roofline   FP64 bound: algorithmic FP64 ops per launch (ope_b200.roofline)
+             / average launch time vs the measured DFMA peak of this GPU.
+  cpu_baseline  the CPU oracle (the reference restated in C++, OpenMP over
+             all host cores) on a bounded sample of the same workload.
+
+``--impl reference`` times that CPU implementation alone (rank 0 only).
+Multi-GPU (torchrun): every rank prices its own 1M-contract shard (weak
+scaling, no collective on the data path); timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import io
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "options-pricing-engine-rs_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "Heston/Bates prices/s batched vs plain, 1 B200, ≤1e-9 err; p50/p99 latency"
+UNIT = "contracts/s"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=1 << 20, help="contracts per rank")
+    ap.add_argument("--plain-surfaces", type=int, default=256)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload(n: int, rank: int):
+    from ope_b200 import workloads as W
+
+    return W.c3(n=n, per_surface=256, seed=3 + rank)
+
+
+def config_of(w, world: int) -> dict:
+    return {
+        "workload": w.name if world == 1 else w.name + "-per-rank",
+        "model": "bates",
+        "n_contracts": w.n,
+        "n_surfaces": w.n_surf,
+        "contracts_per_surface": 256,
+        "tol": w.tol,
+        "max_panels": 200,
+        "parallelism": "replicas" if world > 1 else "single-gpu",
+        "l2": "flushed between timed steps (512 MiB device write); inputs 59 MB < L2",
+    }
+
+
+# ----------------------------------------------------------------- CPU side
+def cpu_sample(w, seconds: float, rng_seed: int = 0):
+    """Time the oracle (all host cores) on a random contract sample sized to ~`seconds`."""
+    from oracle import oracle as O
+
+    O.build()
+    rng = np.random.default_rng(rng_seed)
+    si = w.surf_idx()
+    probe = np.sort(rng.choice(w.n, 2048, replace=False))
+    t0 = time.perf_counter()
+    O.batch_price(w.contracts[probe], w.params, True, w.tol, surf_idx=si[probe])
+    rate = probe.size / (time.perf_counter() - t0)
+    m = int(min(w.n, max(2048, rate * seconds)))
+    idx = np.sort(rng.choice(w.n, m, replace=False))
+    t0 = time.perf_counter()
+    O.batch_price(w.contracts[idx], w.params, True, w.tol, surf_idx=si[idx])
+    dt = time.perf_counter() - t0
+    return m / dt, m, dt, O.max_threads()
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    w = workload(args.n, 0)
+    per_step = max(1.0, min(8.0, 60.0 / max(1, args.steps + args.warmup)))
+    for _ in range(args.warmup):
+        cpu_sample(w, per_step / 4, rng_seed=17)
+    rates, total_m, total_t, cores = [], 0, 0.0, 1
+    for k in range(args.steps):
+        rate, m, dt, cores = cpu_sample(w, per_step, rng_seed=100 + k)
+        rates.append(rate)
+        total_m += m
+        total_t += dt
+    value = total_m / total_t
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total_t / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config_of(w, world),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{total_m} random contracts of the workload over {args.steps} steps "
+                                   f"(~{per_step:.0f} s each), OpenMP dynamic schedule, C++ restatement "
+                                   f"of the reference (no Rust toolchain on this box)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,uuid,utilization.gpu,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str | None):
+        self.uuid = uuid
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"]
+        if self.uuid:
+            cmd[1:1] = ["-i", self.uuid]
+        try:
+            self.p = subprocess.Popen(cmd, stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        time.sleep(0.3)
+
+    def stop(self) -> dict:
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r for r in csv.reader(io.StringIO(self.f.read())) if len(r) >= 11]
+        os.unlink(self.f.name)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            try:
+                util, clk, mx = float(r[2]), float(r[3]), float(r[4])
+            except ValueError:
+                continue
+            smax = mx
+            if util >= 50:
+                sm.append(clk)
+                for nm, v in zip(names, r[7:11]):
+                    if v.lower().startswith("active"):
+                        reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples_under_load": len(sm)}
+
+
+def read_traffic():
+    p = os.path.join(ROOT, "profiles", "c3_persistent_traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("dram_bytes_per_launch_full")
+    return None
+
+
+# ----------------------------------------------------------------- GPU side
+def run_ours(args) -> None:
+    import torch
+
+    import ope_b200 as ope
+    from ope_b200 import roofline
+
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    w = workload(args.n, rank)
+    n, n_surf = w.n, w.n_surf
+    model = ope.MODEL_BATES
+    dev = torch.device("cuda", local_rank)
+    d_con = torch.from_numpy(w.contracts.view(np.uint8).copy()).to(dev)
+    d_off = torch.from_numpy(w.surf_offsets).to(dev)
+    d_par = torch.from_numpy(w.params.copy()).to(dev)
+    d_out = torch.empty(n, dtype=torch.float64, device=dev)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+
+    # untimed: per-integral bisection counts for the work tally
+    nb = np.zeros(2 * n, np.int32)
+    ope.price_surfaces(model, w.contracts, w.surf_offsets, w.params, tol=w.tol, bisections=nb)
+    flops_per_launch = roofline.work_flops(nb, True)
+
+    def step():
+        ope.price_surfaces_device(model, d_con.data_ptr(), n, d_off.data_ptr(), n_surf, d_par.data_ptr(),
+                                  d_out.data_ptr(), tol=w.tol, stream=stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        flush.zero_()
+        step()
+    torch.cuda.synchronize()
+
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(local_rank).uuid)
+    except Exception:
+        pass
+    clocks = ClockSampler(uuid)
+    clocks.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    t_all0, t_all1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    launches0 = ope.kernel_launch_count()
+    t_all0.record(stream)
+    for k in range(args.steps):
+        flush.zero_()
+        ev[k][0].record(stream)
+        step()
+        ev[k][1].record(stream)
+    t_all1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    launches = ope.kernel_launch_count() - launches0
+    clk = clocks.stop()
+    region_ms = max_over_ranks(t_all0.elapsed_time(t_all1))
+    kern_ms = [a.elapsed_time(b) for a, b in ev]
+    kern_avg = statistics.mean(kern_ms)
+    value = world * n * args.steps / (region_ms * 1e-3)
+
+    # check this run's prices against the stats run (same bits expected)
+    ref_prices = np.empty(n)
+    ope.price_surfaces(model, w.contracts, w.surf_offsets, w.params, tol=w.tol, out=ref_prices)
+    assert np.array_equal(d_out.cpu().numpy(), ref_prices), "device-path prices differ from host-path prices"
+
+    # e2e through the public API with pinned host buffers
+    pin_con = torch.empty(n * 56, dtype=torch.uint8, pin_memory=True).numpy().view(w.contracts.dtype)
+    pin_con[:] = w.contracts
+    pin_off = torch.empty(n_surf + 1, dtype=torch.int64, pin_memory=True).numpy()
+    pin_off[:] = w.surf_offsets
+    pin_par = torch.empty((n_surf, 8), dtype=torch.float64, pin_memory=True).numpy()
+    pin_par[:] = w.params
+    pin_out = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    for _ in range(max(1, args.warmup)):
+        ope.price_surfaces(model, pin_con, pin_off, pin_par, tol=w.tol, out=pin_out)
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        ope.price_surfaces(model, pin_con, pin_off, pin_par, tol=w.tol, out=pin_out)
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    barrier()
+    e2e_value = world * n * args.steps / e2e_s
+    h2d = n * 56 + (n_surf + 1) * 8 + n_surf * 8 * 8
+    d2h = n * 8
+
+    # the plain drop-in: one synchronous batch_bates call per surface (host buffers)
+    rng = np.random.default_rng(1000 + rank)
+    picks = np.sort(rng.choice(n_surf, min(args.plain_surfaces, n_surf), replace=False))
+    for s in picks[:8]:
+        ope.batch_bates(w.contracts[w.surf_offsets[s]:w.surf_offsets[s + 1]], w.params[s], tol=w.tol)
+    barrier()
+    t0 = time.perf_counter()
+    cnt = 0
+    for s in picks:
+        c = w.contracts[w.surf_offsets[s]:w.surf_offsets[s + 1]]
+        ope.batch_bates(c, w.params[s], tol=w.tol)
+        cnt += c.size
+    plain_s = max_over_ranks(time.perf_counter() - t0)
+    plain_value = world * cnt / plain_s
+
+    peak_flops, _ = ope.measure_fp64_peak()
+    achieved = flops_per_launch / (kern_avg * 1e-3)
+    traffic = read_traffic()
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": region_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config_of(w, world),
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "api": "ope_price_surfaces (host pointers, pinned)"},
+        "plain": {"value": plain_value, "unit": UNIT, "surfaces_sampled": int(picks.size),
+                  "api": "ope_batch_bates per surface (host pointers, synchronous)",
+                  "batched_e2e_over_plain": e2e_value / plain_value},
+        "roofline": {"bound": "fp64", "achieved": achieved / 1e12, "peak": peak_flops / 1e12, "unit": "TFLOP/s",
+                     "frac": achieved / peak_flops, "traffic": traffic,
+                     "peak_source": "measured DFMA-chain probe on this GPU (ope_measure_fp64_peak)",
+                     "work": f"{flops_per_launch:.4e} FP64 ops per launch = nodes x F_node "
+                             f"(F_node {roofline.F_NODE[(True, True)]}/{roofline.F_NODE[(True, False)]} P1/P2); "
+                             f"nodes/contract {roofline.nodes_total(nb) / n:.1f}",
+                     "kernel_ms": kern_avg},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, m, dt, cores = cpu_sample(w, args.cpu_seconds)
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
+                                "sample": f"{m} random contracts of the workload in {dt:.1f} s"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

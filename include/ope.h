@@ -1,0 +1,159 @@
+/*
+ * ope.h — C ABI of the B200 (sm_100a) Heston/Bates characteristic-function
+ * pricer.  This is the drop-in boundary: the reference crate
+ * (options_pricing_engine 0.1.0, Rust) binds these symbols over `extern "C"`
+ * in place of its CPU pricing path.  Every entry point cites the reference
+ * item it replaces as `file:line` within the reference crate.
+ *
+ * Conventions
+ *  - Every call returns an int status (OPE_OK = 0); nothing aborts.  The
+ *    text of the last error on the calling thread is ope_last_error().
+ *  - Arrays are caller-owned.  Plain calls take HOST pointers and return
+ *    once results are in the caller's buffer.  With OPE_FLAG_DEVICE_PTRS in
+ *    ope_options.flags every array argument is a DEVICE pointer and the call
+ *    is stream-ordered on ope_options.stream (it returns after enqueueing).
+ *  - All arithmetic is IEEE binary64.  The quadrature is the reference's
+ *    greedy globally-adaptive Gauss-Kronrod-15 with at most 200 live panels
+ *    (heston.rs:193-212); the absolute tolerance defaults to the reference's
+ *    hard-coded 1e-8 (heston.rs:228) and is settable through ope_options.tol.
+ *  - Thread safety: calls may come from any host thread.  Each thread owns
+ *    a private device workspace; asynchronous (device-pointer) calls issued
+ *    from ONE thread on DIFFERENT streams must not overlap in time, because
+ *    they share that thread's workspace.
+ *  - Single GPU: the current CUDA device of the calling thread.
+ */
+#ifndef OPE_H
+#define OPE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+enum {
+    OPE_OK = 0,
+    OPE_ERR_INVALID_ARG = 1,   /* NULL pointer, n/size mismatch, bad enum, tol not finite */
+    OPE_ERR_OUT_OF_MEMORY = 2, /* device allocation failed */
+    OPE_ERR_DEVICE = 3,        /* CUDA runtime/kernel error (see ope_last_error) */
+    OPE_ERR_NO_DEVICE = 4,     /* no CUDA device, or the device is not sm_100 */
+    OPE_ERR_TIMEOUT = 5,       /* a bounded device/host wait expired */
+    OPE_ERR_REJECTED = 6,      /* admission control refused the request (serving) */
+    OPE_ERR_CANCELLED = 7,     /* request cancelled before completion (serving) */
+    OPE_ERR_NOT_FOUND = 8      /* unknown request id (serving) */
+};
+
+enum { OPE_CALL = 0, OPE_PUT = 1 };                /* types.rs:5-13 OptionType */
+enum { OPE_MODEL_HESTON = 0, OPE_MODEL_BATES = 1 };
+
+#define OPE_REF_TOL 1e-8          /* heston.rs:228 */
+#define OPE_MAX_PANELS 200        /* heston.rs:194 */
+#define OPE_FLAG_DEVICE_PTRS 1u
+
+/* ------------------------------------------------------------- records */
+/* types.rs:16-25 OptionContract (`vol` is carried but unused by Heston/Bates,
+ * exactly as in batch.rs:25; it seeds the IV solver in calibration). 56 B. */
+typedef struct {
+    double spot, strike, expiry, rate, div_yield, vol;
+    int32_t opt_type; /* OPE_CALL / OPE_PUT */
+    int32_t pad;
+} ope_contract;
+
+/* types.rs:48-54 HestonParams (v0 is a variance). 40 B. */
+typedef struct {
+    double v0, kappa, theta, sigma, rho;
+} ope_heston_params;
+
+/* types.rs:66-72 BatesParams. 64 B. */
+typedef struct {
+    ope_heston_params heston;
+    double lambda, mu_j, sigma_j;
+} ope_bates_params;
+
+/* types.rs:29-39 PricingResult. 64 B. */
+typedef struct {
+    double price, delta, gamma, vega, theta, rho, vanna, volga;
+} ope_pricing_result;
+
+typedef struct {
+    double tol;        /* absolute GK15 tolerance; <= 0 selects OPE_REF_TOL */
+    uint32_t flags;    /* OPE_FLAG_DEVICE_PTRS */
+    uint32_t reserved;
+    void* stream;      /* cudaStream_t; used with OPE_FLAG_DEVICE_PTRS; NULL = default stream */
+} ope_options;
+
+/* ------------------------------------------------ library / diagnostics */
+const char* ope_last_error(void);            /* thread-local text of the last failure */
+const char* ope_version(void);
+int ope_device_info(int32_t* sm_count, int32_t* cc_major, int32_t* cc_minor);
+/* Device kernels launched by this library on the calling thread since load. */
+uint64_t ope_kernel_launch_count(void);
+
+/* ------------------------------------------------ reference drop-ins */
+/* heston.rs:61-72 heston_price.  One contract. */
+int ope_heston_price(double spot, double strike, double expiry, double rate, double div_yield,
+                     const ope_heston_params* params, int32_t opt_type, double* out_price);
+
+/* bates.rs:29-39 bates_price. */
+int ope_bates_price(double spot, double strike, double expiry, double rate, double div_yield,
+                    const ope_bates_params* params, int32_t opt_type, double* out_price);
+
+/* batch.rs:23-27 batch_heston: one parameter set for the whole slice; output
+ * in input order.  The "plain per-surface" launch: one warp per integral. */
+int ope_batch_heston(const ope_contract* contracts, size_t n, const ope_heston_params* params,
+                     double* out_prices);
+
+/* batch.rs:38-42 batch_bates. */
+int ope_batch_bates(const ope_contract* contracts, size_t n, const ope_bates_params* params,
+                    double* out_prices);
+
+/* batch.rs:32-36 batch_heston_greeks (greeks.rs:19-72 bump-and-reprice: 14
+ * pricings per contract, priced as extra work units in one launch). */
+int ope_batch_heston_greeks(const ope_contract* contracts, size_t n, const ope_heston_params* params,
+                            ope_pricing_result* out);
+
+/* batch.rs:44-48 batch_bates_greeks. */
+int ope_batch_bates_greeks(const ope_contract* contracts, size_t n, const ope_bates_params* params,
+                           ope_pricing_result* out);
+
+/* The two batch entry points above with explicit options (tolerance, device
+ * pointers, stream).  `model` selects the params type. */
+int ope_batch_price_ex(int32_t model, const ope_contract* contracts, size_t n, const void* params,
+                       double* out_prices, const ope_options* opts);
+
+/* batch.rs:32-36 / 44-48 with explicit options (tolerance, device pointers,
+ * stream); the reference's greeks always use the 1e-8 tolerance. */
+int ope_batch_greeks_ex(int32_t model, const ope_contract* contracts, size_t n, const void* params,
+                        ope_pricing_result* out, const ope_options* opts);
+
+/* --------------------------------------- batched multi-surface pricing */
+/* No single reference twin: many batch_heston/batch_bates calls (batch.rs:23,
+ * 38), one per surface, fused into ONE persistent launch.  Surface s owns
+ * contracts [surf_offsets[s], surf_offsets[s+1]) and prices them with
+ * params[s] (ope_heston_params[] or ope_bates_params[] by `model`).
+ * surf_offsets has n_surf+1 entries, starts at 0, ends at n, non-decreasing.
+ * A device work queue hands (contract, integral) units to warps. */
+int ope_price_surfaces(int32_t model, const ope_contract* contracts, size_t n,
+                       const int64_t* surf_offsets, size_t n_surf, const void* params,
+                       double* out_prices, const ope_options* opts);
+
+/* ope_price_surfaces plus diagnostics: out_bisections (may be NULL) receives
+ * 2n int32 — the bisection count of each contract's P1 and P2 integral (the
+ * loop iterations of heston.rs:200-210), from which the nodes evaluated are
+ * 15 * (1 + 2 * count). */
+int ope_price_surfaces_stats(int32_t model, const ope_contract* contracts, size_t n,
+                             const int64_t* surf_offsets, size_t n_surf, const void* params,
+                             double* out_prices, int32_t* out_bisections, const ope_options* opts);
+
+/* No reference twin (measurement support): the FP64 throughput of this GPU,
+ * measured by a DFMA-chain kernel (2 flops per DFMA) on the calling thread's
+ * device.  The roofline denominator for the FP64-bound pricing kernels. */
+int ope_measure_fp64_peak(double* flops_per_s, double* elapsed_ms);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* OPE_H */

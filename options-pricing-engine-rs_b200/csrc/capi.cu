@@ -1,0 +1,304 @@
+// C-ABI implementation (include/ope.h): per-thread context, argument
+// validation, host<->device staging and dispatch to the kernels.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "internal.h"
+
+namespace ope {
+
+ThreadCtx& tctx() {
+    static thread_local ThreadCtx c;
+    return c;
+}
+
+int set_error(int code, const std::string& msg) {
+    tctx().last_error = msg;
+    return code;
+}
+
+int check_cuda(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return OPE_OK;
+    std::string msg = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+    if (e == cudaErrorMemoryAllocation) return set_error(OPE_ERR_OUT_OF_MEMORY, msg);
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return set_error(OPE_ERR_NO_DEVICE, msg);
+    return set_error(OPE_ERR_DEVICE, msg);
+}
+
+int ensure_device() {
+    ThreadCtx& c = tctx();
+    int cur = -1;
+    cudaError_t e = cudaGetDevice(&cur);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(OPE_ERR_NO_DEVICE, std::string("no CUDA device: ") + cudaGetErrorString(e));
+    }
+    if (c.device == cur) return OPE_OK;
+    int major = 0, minor = 0, sms = 0;
+    OPE_CHECK(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, cur));
+    OPE_CHECK(cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, cur));
+    OPE_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, cur));
+    if (major != 10 || minor != 0) {
+        return set_error(OPE_ERR_NO_DEVICE, "this library is built for sm_100a (B200); device " + std::to_string(cur) +
+                                                " is sm_" + std::to_string(major) + std::to_string(minor));
+    }
+    // A new device for this thread: drop the old device's resources (leaked
+    // rather than freed on the wrong device).
+    c.ws = nullptr;
+    c.ws_bytes = 0;
+    OPE_CHECK(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+    c.device = cur;
+    c.sm_count = sms;
+    c.cc_major = major;
+    c.cc_minor = minor;
+    return OPE_OK;
+}
+
+int ensure_workspace(size_t bytes, void** out) {
+    ThreadCtx& c = tctx();
+    if (bytes > c.ws_bytes) {
+        if (c.ws) {
+            OPE_CHECK(cudaDeviceSynchronize());
+            OPE_CHECK(cudaFree(c.ws));
+            c.ws = nullptr;
+            c.ws_bytes = 0;
+        }
+        size_t want = std::max(bytes, c.ws_bytes + c.ws_bytes / 2);
+        want = align_up(want, 1 << 20);
+        OPE_CHECK(cudaMalloc(&c.ws, want));
+        c.ws_bytes = want;
+    }
+    *out = c.ws;
+    return OPE_OK;
+}
+
+int ensure_pinned(size_t bytes, void** out) {
+    ThreadCtx& c = tctx();
+    if (bytes > c.pinned_bytes) {
+        if (c.pinned) {
+            OPE_CHECK(cudaFreeHost(c.pinned));
+            c.pinned = nullptr;
+            c.pinned_bytes = 0;
+        }
+        size_t want = align_up(std::max(bytes, (size_t)1 << 20), 1 << 20);
+        OPE_CHECK(cudaMallocHost(&c.pinned, want));
+        c.pinned_bytes = want;
+    }
+    *out = c.pinned;
+    return OPE_OK;
+}
+
+namespace {
+
+int resolve_tol(const ope_options* o, double* tol) {
+    double t = (o && o->tol > 0.0) ? o->tol : OPE_REF_TOL;
+    if (o && std::isnan(o->tol)) return set_error(OPE_ERR_INVALID_ARG, "tol is NaN");
+    if (!std::isfinite(t)) return set_error(OPE_ERR_INVALID_ARG, "tol must be finite");
+    *tol = t;
+    return OPE_OK;
+}
+
+int check_model(int32_t model) {
+    if (model != OPE_MODEL_HESTON && model != OPE_MODEL_BATES)
+        return set_error(OPE_ERR_INVALID_ARG, "model must be OPE_MODEL_HESTON or OPE_MODEL_BATES");
+    return OPE_OK;
+}
+
+bool device_ptrs(const ope_options* o) { return o && (o->flags & OPE_FLAG_DEVICE_PTRS); }
+cudaStream_t user_stream(const ope_options* o) { return o ? static_cast<cudaStream_t>(o->stream) : nullptr; }
+
+// Plain (one parameter set) pricing, host or device pointers.
+int batch_price(int32_t model, const ope_contract* contracts, size_t n, const void* params, double* out,
+                const ope_options* opts) {
+    OPE_TRY(check_model(model));
+    double tol;
+    OPE_TRY(resolve_tol(opts, &tol));
+    if (n == 0) return OPE_OK;
+    if (!contracts || !params || !out) return set_error(OPE_ERR_INVALID_ARG, "NULL array argument");
+    OPE_TRY(ensure_device());
+    const int stride = param_stride(model);
+    if (device_ptrs(opts)) {
+        void* ws;
+        OPE_TRY(ensure_workspace(price_scratch_bytes(n), &ws));
+        return launch_price_plain(model, contracts, n, static_cast<const double*>(params), tol, out,
+                                  carve_price_scratch(ws, n), user_stream(opts));
+    }
+    ThreadCtx& c = tctx();
+    const size_t b_con = align_up(n * sizeof(ope_contract), 256), b_par = 256, b_out = align_up(n * sizeof(double), 256);
+    void* ws;
+    OPE_TRY(ensure_workspace(b_con + b_par + b_out + price_scratch_bytes(n), &ws));
+    char* p = static_cast<char*>(ws);
+    ope_contract* d_con = reinterpret_cast<ope_contract*>(p);
+    double* d_par = reinterpret_cast<double*>(p + b_con);
+    double* d_out = reinterpret_cast<double*>(p + b_con + b_par);
+    void* scratch = p + b_con + b_par + b_out;
+    OPE_CHECK(cudaMemcpyAsync(d_con, contracts, n * sizeof(ope_contract), cudaMemcpyHostToDevice, c.stream));
+    OPE_CHECK(cudaMemcpyAsync(d_par, params, stride * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    OPE_TRY(launch_price_plain(model, d_con, n, d_par, tol, d_out, carve_price_scratch(scratch, n), c.stream));
+    OPE_CHECK(cudaMemcpyAsync(out, d_out, n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    OPE_CHECK(cudaStreamSynchronize(c.stream));
+    return OPE_OK;
+}
+
+int batch_greeks(int32_t model, const ope_contract* contracts, size_t n, const void* params,
+                 ope_pricing_result* out, const ope_options* opts) {
+    OPE_TRY(check_model(model));
+    double tol;
+    OPE_TRY(resolve_tol(opts, &tol));
+    if (n == 0) return OPE_OK;
+    if (!contracts || !params || !out) return set_error(OPE_ERR_INVALID_ARG, "NULL array argument");
+    OPE_TRY(ensure_device());
+    const int stride = param_stride(model);
+    if (device_ptrs(opts)) {
+        void* ws;
+        OPE_TRY(ensure_workspace(greeks_workspace_bytes(n), &ws));
+        return launch_greeks(model, contracts, n, static_cast<const double*>(params), tol, out, ws, user_stream(opts));
+    }
+    ThreadCtx& c = tctx();
+    const size_t b_con = align_up(n * sizeof(ope_contract), 256), b_par = 256,
+                 b_out = align_up(n * sizeof(ope_pricing_result), 256);
+    void* ws;
+    OPE_TRY(ensure_workspace(b_con + b_par + b_out + greeks_workspace_bytes(n), &ws));
+    char* p = static_cast<char*>(ws);
+    ope_contract* d_con = reinterpret_cast<ope_contract*>(p);
+    double* d_par = reinterpret_cast<double*>(p + b_con);
+    ope_pricing_result* d_out = reinterpret_cast<ope_pricing_result*>(p + b_con + b_par);
+    void* gws = p + b_con + b_par + b_out;
+    OPE_CHECK(cudaMemcpyAsync(d_con, contracts, n * sizeof(ope_contract), cudaMemcpyHostToDevice, c.stream));
+    OPE_CHECK(cudaMemcpyAsync(d_par, params, stride * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    OPE_TRY(launch_greeks(model, d_con, n, d_par, tol, d_out, gws, c.stream));
+    OPE_CHECK(cudaMemcpyAsync(out, d_out, n * sizeof(ope_pricing_result), cudaMemcpyDeviceToHost, c.stream));
+    OPE_CHECK(cudaStreamSynchronize(c.stream));
+    return OPE_OK;
+}
+
+}  // namespace
+}  // namespace ope
+
+using namespace ope;
+
+extern "C" {
+
+const char* ope_last_error(void) { return tctx().last_error.c_str(); }
+
+const char* ope_version(void) { return "ope-b200 0.1.0 (sm_100a, FP64 greedy GK15)"; }
+
+uint64_t ope_kernel_launch_count(void) { return tctx().launches; }
+
+int ope_device_info(int32_t* sm_count, int32_t* cc_major, int32_t* cc_minor) {
+    OPE_TRY(ensure_device());
+    if (sm_count) *sm_count = tctx().sm_count;
+    if (cc_major) *cc_major = tctx().cc_major;
+    if (cc_minor) *cc_minor = tctx().cc_minor;
+    return OPE_OK;
+}
+
+int ope_heston_price(double spot, double strike, double expiry, double rate, double div_yield,
+                     const ope_heston_params* params, int32_t opt_type, double* out_price) {
+    if (!params || !out_price) return set_error(OPE_ERR_INVALID_ARG, "NULL argument");
+    if (opt_type != OPE_CALL && opt_type != OPE_PUT) return set_error(OPE_ERR_INVALID_ARG, "bad opt_type");
+    ope_contract c{spot, strike, expiry, rate, div_yield, 0.0, opt_type, 0};
+    return batch_price(OPE_MODEL_HESTON, &c, 1, params, out_price, nullptr);
+}
+
+int ope_bates_price(double spot, double strike, double expiry, double rate, double div_yield,
+                    const ope_bates_params* params, int32_t opt_type, double* out_price) {
+    if (!params || !out_price) return set_error(OPE_ERR_INVALID_ARG, "NULL argument");
+    if (opt_type != OPE_CALL && opt_type != OPE_PUT) return set_error(OPE_ERR_INVALID_ARG, "bad opt_type");
+    ope_contract c{spot, strike, expiry, rate, div_yield, 0.0, opt_type, 0};
+    return batch_price(OPE_MODEL_BATES, &c, 1, params, out_price, nullptr);
+}
+
+int ope_batch_heston(const ope_contract* contracts, size_t n, const ope_heston_params* params, double* out) {
+    return batch_price(OPE_MODEL_HESTON, contracts, n, params, out, nullptr);
+}
+
+int ope_batch_bates(const ope_contract* contracts, size_t n, const ope_bates_params* params, double* out) {
+    return batch_price(OPE_MODEL_BATES, contracts, n, params, out, nullptr);
+}
+
+int ope_batch_heston_greeks(const ope_contract* contracts, size_t n, const ope_heston_params* params,
+                            ope_pricing_result* out) {
+    return batch_greeks(OPE_MODEL_HESTON, contracts, n, params, out, nullptr);
+}
+
+int ope_batch_bates_greeks(const ope_contract* contracts, size_t n, const ope_bates_params* params,
+                           ope_pricing_result* out) {
+    return batch_greeks(OPE_MODEL_BATES, contracts, n, params, out, nullptr);
+}
+
+int ope_batch_price_ex(int32_t model, const ope_contract* contracts, size_t n, const void* params,
+                       double* out_prices, const ope_options* opts) {
+    return batch_price(model, contracts, n, params, out_prices, opts);
+}
+
+int ope_batch_greeks_ex(int32_t model, const ope_contract* contracts, size_t n, const void* params,
+                        ope_pricing_result* out, const ope_options* opts) {
+    return batch_greeks(model, contracts, n, params, out, opts);
+}
+
+int ope_measure_fp64_peak(double* flops_per_s, double* elapsed_ms) {
+    if (!flops_per_s || !elapsed_ms) return set_error(OPE_ERR_INVALID_ARG, "NULL argument");
+    OPE_TRY(ensure_device());
+    return measure_fp64_peak(flops_per_s, elapsed_ms);
+}
+
+int ope_price_surfaces(int32_t model, const ope_contract* contracts, size_t n, const int64_t* surf_offsets,
+                       size_t n_surf, const void* params, double* out_prices, const ope_options* opts) {
+    return ope_price_surfaces_stats(model, contracts, n, surf_offsets, n_surf, params, out_prices, nullptr, opts);
+}
+
+int ope_price_surfaces_stats(int32_t model, const ope_contract* contracts, size_t n, const int64_t* surf_offsets,
+                             size_t n_surf, const void* params, double* out_prices, int32_t* out_bisections,
+                             const ope_options* opts) {
+    OPE_TRY(check_model(model));
+    double tol;
+    OPE_TRY(resolve_tol(opts, &tol));
+    if (n == 0) return OPE_OK;
+    if (!contracts || !params || !out_prices || !surf_offsets)
+        return set_error(OPE_ERR_INVALID_ARG, "NULL array argument");
+    if (n_surf == 0) return set_error(OPE_ERR_INVALID_ARG, "n_surf must be >= 1 when n > 0");
+    OPE_TRY(ensure_device());
+    const int stride = param_stride(model);
+    if (device_ptrs(opts)) {
+        void* ws;
+        OPE_TRY(ensure_workspace(price_scratch_bytes(n), &ws));
+        return launch_price_persistent(model, contracts, n, surf_offsets, n_surf, nullptr,
+                                       static_cast<const double*>(params), tol, out_prices, carve_price_scratch(ws, n),
+                                       user_stream(opts), out_bisections);
+    }
+    if (surf_offsets[0] != 0 || surf_offsets[n_surf] != (int64_t)n)
+        return set_error(OPE_ERR_INVALID_ARG, "surf_offsets must start at 0 and end at n");
+    for (size_t s = 0; s < n_surf; ++s)
+        if (surf_offsets[s + 1] < surf_offsets[s]) return set_error(OPE_ERR_INVALID_ARG, "surf_offsets not sorted");
+    ThreadCtx& c = tctx();
+    const size_t b_con = align_up(n * sizeof(ope_contract), 256), b_off = align_up((n_surf + 1) * sizeof(int64_t), 256),
+                 b_par = align_up(n_surf * stride * sizeof(double), 256), b_out = align_up(n * sizeof(double), 256),
+                 b_nb = out_bisections ? align_up(2 * n * sizeof(int32_t), 256) : 0;
+    void* ws;
+    OPE_TRY(ensure_workspace(b_con + b_off + b_par + b_out + b_nb + price_scratch_bytes(n), &ws));
+    char* p = static_cast<char*>(ws);
+    ope_contract* d_con = reinterpret_cast<ope_contract*>(p);
+    int64_t* d_off = reinterpret_cast<int64_t*>(p + b_con);
+    double* d_par = reinterpret_cast<double*>(p + b_con + b_off);
+    double* d_out = reinterpret_cast<double*>(p + b_con + b_off + b_par);
+    int32_t* d_nb = out_bisections ? reinterpret_cast<int32_t*>(p + b_con + b_off + b_par + b_out) : nullptr;
+    void* scratch = p + b_con + b_off + b_par + b_out + b_nb;
+    OPE_CHECK(cudaMemcpyAsync(d_con, contracts, n * sizeof(ope_contract), cudaMemcpyHostToDevice, c.stream));
+    OPE_CHECK(cudaMemcpyAsync(d_off, surf_offsets, (n_surf + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, c.stream));
+    OPE_CHECK(cudaMemcpyAsync(d_par, params, n_surf * stride * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    OPE_TRY(launch_price_persistent(model, d_con, n, d_off, n_surf, nullptr, d_par, tol, d_out,
+                                    carve_price_scratch(scratch, n), c.stream, d_nb));
+    OPE_CHECK(cudaMemcpyAsync(out_prices, d_out, n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    if (out_bisections)
+        OPE_CHECK(cudaMemcpyAsync(out_bisections, d_nb, 2 * n * sizeof(int32_t), cudaMemcpyDeviceToHost, c.stream));
+    OPE_CHECK(cudaStreamSynchronize(c.stream));
+    return OPE_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,81 @@
+// Internal host-side interfaces shared by the C-ABI translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/ope.h"
+
+namespace ope {
+
+// Per-thread library state: current device, an internal stream for the
+// synchronous host-pointer calls, a growable device workspace and the text
+// of the last error.  Thread-local so concurrent host threads never share a
+// workspace.
+struct ThreadCtx {
+    int device = -1;
+    int sm_count = 0;
+    int cc_major = 0, cc_minor = 0;
+    cudaStream_t stream = nullptr;
+    void* ws = nullptr;      // device workspace
+    size_t ws_bytes = 0;
+    void* pinned = nullptr;  // pinned host staging
+    size_t pinned_bytes = 0;
+    std::string last_error;
+    uint64_t launches = 0;
+};
+
+ThreadCtx& tctx();
+int set_error(int code, const std::string& msg);
+int check_cuda(cudaError_t e, const char* what);
+int ensure_device();                               // OPE_OK or OPE_ERR_NO_DEVICE
+int ensure_workspace(size_t bytes, void** out);    // grows the per-thread workspace
+int ensure_pinned(size_t bytes, void** out);       // grows the pinned staging buffer
+
+#define OPE_CHECK(call)                                        \
+    do {                                                       \
+        int _rc = ::ope::check_cuda((call), #call);            \
+        if (_rc != OPE_OK) return _rc;                         \
+    } while (0)
+
+#define OPE_TRY(expr)                                          \
+    do {                                                       \
+        int _rc = (expr);                                      \
+        if (_rc != OPE_OK) return _rc;                         \
+    } while (0)
+
+inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+// Scratch needed by one pricing launch over n contracts: per-contract integral
+// pair + completion counter, and the work-queue head.
+struct PriceScratch {
+    double* integ;            // 2n
+    unsigned int* done;       // n   (must be zero before launch)
+    unsigned long long* head; // 1   (must be zero before launch; persistent only)
+};
+size_t price_scratch_bytes(size_t n);
+PriceScratch carve_price_scratch(void* base, size_t n);
+
+// Device launchers (stream-ordered; all pointers are device pointers).
+int launch_price_plain(int model, const ope_contract* con, size_t n, const double* params, double tol,
+                       double* out, const PriceScratch& s, cudaStream_t st, int32_t* nbis_out = nullptr);
+// Contract c is priced with params + stride * p(c), where p(c) = param_idx[c]
+// when param_idx is non-NULL, else the surface of c under surf_offsets
+// (n_surf + 1 entries), else 0.
+int launch_price_persistent(int model, const ope_contract* con, size_t n, const int64_t* surf_offsets,
+                            size_t n_surf, const int32_t* param_idx, const double* params, double tol, double* out,
+                            const PriceScratch& s, cudaStream_t st, int32_t* nbis_out = nullptr);
+// DFMA throughput probe: FP64 flop/s (2 per FMA) over ~`ms_target` ms.
+int measure_fp64_peak(double* flops, double* ms);
+// Bump-and-reprice Greeks (greeks.rs:19-72) for n contracts under one
+// parameter set; `ws` must hold greeks_workspace_bytes(n) bytes.
+size_t greeks_workspace_bytes(size_t n);
+int launch_greeks(int model, const ope_contract* con, size_t n, const double* params, double tol,
+                  ope_pricing_result* out, void* ws, cudaStream_t st);
+
+inline int param_stride(int model) { return model == OPE_MODEL_BATES ? 8 : 5; }
+
+}  // namespace ope

@@ -1,0 +1,192 @@
+// Pricing kernels: the plain per-surface launch (batch.rs:23-42 drop-in) and
+// the persistent multi-surface launch with a device work queue.
+//
+// Work unit = one Gil-Pelaez integral of one contract (P1 or P2,
+// heston.rs:92-93 / bates.rs:58-59), integrated by one warp.  The two
+// integrals of a contract run on different warps; whichever finishes second
+// combines them into the price (heston.rs:95-98) through a per-contract
+// completion counter.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "internal.h"
+#include "quadrature.cuh"
+
+namespace ope {
+
+size_t price_scratch_bytes(size_t n) {
+    return align_up(2 * n * sizeof(double), 256) + align_up(n * sizeof(unsigned int), 256) + 256;
+}
+
+PriceScratch carve_price_scratch(void* base, size_t n) {
+    char* p = static_cast<char*>(base);
+    PriceScratch s;
+    s.integ = reinterpret_cast<double*>(p);
+    p += align_up(2 * n * sizeof(double), 256);
+    s.done = reinterpret_cast<unsigned int*>(p);
+    p += align_up(n * sizeof(unsigned int), 256);
+    s.head = reinterpret_cast<unsigned long long*>(p);
+    return s;
+}
+
+namespace {
+
+struct ContractView {
+    double s, k, t, r, q;
+    int opt_type;
+};
+
+__device__ __forceinline__ ContractView load_contract(const ope_contract* con, long long c) {
+    const ope_contract* p = con + c;
+    ContractView v;
+    v.s = __ldg(&p->spot);
+    v.k = __ldg(&p->strike);
+    v.t = __ldg(&p->expiry);
+    v.r = __ldg(&p->rate);
+    v.q = __ldg(&p->div_yield);
+    v.opt_type = __ldg(&p->opt_type);
+    return v;
+}
+
+// Integrate unit (contract c, integral `which`) and, if it completes the
+// contract, write the price.
+template <bool BATES>
+__device__ __forceinline__ void run_unit(long long c, int which, const ope_contract* con, const double* p,
+                                         double tol, double* out, double* integ, unsigned int* done,
+                                         int32_t* nbis_out, PanelStore& L, int lane, const LaneRule& R) {
+    const ContractView v = load_contract(con, c);
+    double pl[8];
+#pragma unroll
+    for (int i = 0; i < (BATES ? 8 : 5); ++i) pl[i] = __ldg(p + i);
+    const CfConsts C = make_consts(v.s, v.k, v.t, v.r, pl, BATES, which);
+    int nb;
+    const double I = gk_integrate_warp<BATES>(C, tol, L, lane, R, &nb);
+    if (lane == 0) {
+        if (nbis_out) nbis_out[2 * c + which] = nb;
+        integ[2 * c + which] = I;
+        __threadfence();
+        const unsigned int prev = atomicAdd(done + c, 1u);
+        if (prev == 1u) {
+            __threadfence();
+            const double other = __ldcg(integ + 2 * c + (1 - which));
+            const double i1 = which == 0 ? I : other;
+            const double i2 = which == 0 ? other : I;
+            out[c] = finish_price(v.s, v.k, v.t, v.r, v.q, v.opt_type, i1, i2);
+        }
+    }
+}
+
+// Plain launch: one warp per unit, one parameter set (a single batch_* call).
+template <bool BATES>
+__global__ void __launch_bounds__(128) k_price_plain(const ope_contract* __restrict__ con, long long n,
+                                                     const double* __restrict__ params, double tol,
+                                                     double* __restrict__ out, double* integ,
+                                                     unsigned int* done, int32_t* nbis_out) {
+    extern __shared__ PanelStore smem_panels[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long unit = (long long)blockIdx.x * (blockDim.x >> 5) + warp;
+    if (unit >= 2 * n) return;
+    const LaneRule R = lane_rule(lane);
+    run_unit<BATES>(unit >> 1, (int)(unit & 1), con, params, tol, out, integ, done, nbis_out, smem_panels[warp],
+                    lane, R);
+}
+
+// Surface of contract c: the s with off[s] <= c < off[s+1] (upper_bound - 1).
+__device__ __forceinline__ long long find_surface(const int64_t* off, long long n_surf, long long c) {
+    long long lo = 1, hi = n_surf;  // search [1, n_surf] for the first off[j] > c
+    while (lo < hi) {
+        const long long mid = (lo + hi) >> 1;
+        if (__ldg(off + mid) > c) hi = mid; else lo = mid + 1;
+    }
+    return lo - 1;
+}
+
+// Persistent launch: a grid sized to the resident capacity; every warp pulls
+// units from the device queue until it drains.
+template <bool BATES>
+__global__ void __launch_bounds__(128) k_price_persistent(const ope_contract* __restrict__ con, long long n,
+                                                          const int64_t* __restrict__ surf_off, long long n_surf,
+                                                          const int32_t* __restrict__ param_idx,
+                                                          const double* __restrict__ params, double tol,
+                                                          double* __restrict__ out, double* integ,
+                                                          unsigned int* done, unsigned long long* head,
+                                                          int32_t* nbis_out) {
+    extern __shared__ PanelStore smem_panels[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const LaneRule R = lane_rule(lane);
+    const int stride = BATES ? 8 : 5;
+    const unsigned long long n_units = 2ull * (unsigned long long)n;
+    while (true) {
+        unsigned long long unit = 0;
+        if (lane == 0) unit = atomicAdd(head, 1ull);
+        unit = __shfl_sync(0xffffffffu, unit, 0);
+        if (unit >= n_units) break;
+        const long long c = (long long)(unit >> 1);
+        const long long s = param_idx ? (long long)__ldg(param_idx + c)
+                                      : (n_surf > 1 ? find_surface(surf_off, n_surf, c) : 0);
+        run_unit<BATES>(c, (int)(unit & 1), con, params + s * stride, tol, out, integ, done, nbis_out,
+                        smem_panels[warp], lane, R);
+    }
+}
+
+template <class K>
+int persistent_grid(K kernel, int threads, size_t smem, int* grid) {
+    int per_sm = 0;
+    OPE_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    OPE_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem));
+    if (per_sm < 1) per_sm = 1;
+    *grid = per_sm * tctx().sm_count;
+    return OPE_OK;
+}
+
+}  // namespace
+
+int launch_price_plain(int model, const ope_contract* con, size_t n, const double* params, double tol,
+                       double* out, const PriceScratch& s, cudaStream_t st, int32_t* nbis_out) {
+    if (n == 0) return OPE_OK;
+    OPE_CHECK(cudaMemsetAsync(s.done, 0, n * sizeof(unsigned int), st));
+    const int warps = 4, threads = warps * 32;
+    const size_t smem = warps * sizeof(PanelStore);
+    const unsigned long long units = 2ull * n;
+    const unsigned int grid = (unsigned int)((units + warps - 1) / warps);
+    if (model == OPE_MODEL_BATES) {
+        OPE_CHECK(cudaFuncSetAttribute(k_price_plain<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_price_plain<true><<<grid, threads, smem, st>>>(con, (long long)n, params, tol, out, s.integ, s.done, nbis_out);
+    } else {
+        OPE_CHECK(cudaFuncSetAttribute(k_price_plain<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_price_plain<false><<<grid, threads, smem, st>>>(con, (long long)n, params, tol, out, s.integ, s.done, nbis_out);
+    }
+    OPE_CHECK(cudaGetLastError());
+    tctx().launches += 1;
+    return OPE_OK;
+}
+
+int launch_price_persistent(int model, const ope_contract* con, size_t n, const int64_t* surf_offsets,
+                            size_t n_surf, const int32_t* param_idx, const double* params, double tol, double* out,
+                            const PriceScratch& s, cudaStream_t st, int32_t* nbis_out) {
+    if (n == 0) return OPE_OK;
+    OPE_CHECK(cudaMemsetAsync(s.done, 0, n * sizeof(unsigned int), st));
+    OPE_CHECK(cudaMemsetAsync(s.head, 0, sizeof(unsigned long long), st));
+    const int warps = 4, threads = warps * 32;
+    const size_t smem = warps * sizeof(PanelStore);
+    int grid = 0;
+    if (model == OPE_MODEL_BATES) {
+        OPE_TRY(persistent_grid(k_price_persistent<true>, threads, smem, &grid));
+        const unsigned long long need = (2ull * n + warps - 1) / warps;
+        grid = (int)std::min<unsigned long long>((unsigned long long)grid, need);
+        k_price_persistent<true><<<grid, threads, smem, st>>>(con, (long long)n, surf_offsets, (long long)n_surf,
+                                                              param_idx, params, tol, out, s.integ, s.done, s.head, nbis_out);
+    } else {
+        OPE_TRY(persistent_grid(k_price_persistent<false>, threads, smem, &grid));
+        const unsigned long long need = (2ull * n + warps - 1) / warps;
+        grid = (int)std::min<unsigned long long>((unsigned long long)grid, need);
+        k_price_persistent<false><<<grid, threads, smem, st>>>(con, (long long)n, surf_offsets, (long long)n_surf,
+                                                               param_idx, params, tol, out, s.integ, s.done, s.head, nbis_out);
+    }
+    OPE_CHECK(cudaGetLastError());
+    tctx().launches += 1;
+    return OPE_OK;
+}
+
+}  // namespace ope

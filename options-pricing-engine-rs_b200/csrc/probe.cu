@@ -1,0 +1,54 @@
+// FP64 throughput probe: the denominator of the pricing kernel's roofline.
+//
+// The pricing path is bound by the FP64 pipe of the CUDA cores (no tensor
+// core work, negligible HBM traffic), and no FP64 figure is published for
+// this pool, so the library measures it: every thread runs eight independent
+// DFMA chains (enough ILP to saturate the pipe) over a grid of 32 resident
+// warps per SM, timed with CUDA events.  Counted as 2 flops per DFMA.
+#include <cuda_runtime.h>
+
+#include "internal.h"
+
+namespace ope {
+namespace {
+
+__global__ void __launch_bounds__(256) k_dfma_probe(double b, double c, int iters, double* sink) {
+    double a0 = threadIdx.x * 1e-9, a1 = a0 + 1e-9, a2 = a0 + 2e-9, a3 = a0 + 3e-9;
+    double a4 = a0 + 4e-9, a5 = a0 + 5e-9, a6 = a0 + 6e-9, a7 = a0 + 7e-9;
+    for (int i = 0; i < iters; ++i) {
+        a0 = fma(a0, b, c); a1 = fma(a1, b, c); a2 = fma(a2, b, c); a3 = fma(a3, b, c);
+        a4 = fma(a4, b, c); a5 = fma(a5, b, c); a6 = fma(a6, b, c); a7 = fma(a7, b, c);
+    }
+    const double s = ((a0 + a1) + (a2 + a3)) + ((a4 + a5) + (a6 + a7));
+    if (s == 1234.5678) sink[0] = s;  // never true; keeps the chains live
+}
+
+}  // namespace
+
+int measure_fp64_peak(double* flops, double* ms) {
+    ThreadCtx& c = tctx();
+    void* ws;
+    OPE_TRY(ensure_workspace(256, &ws));
+    const int threads = 256, blocks = c.sm_count * 4;
+    cudaEvent_t e0, e1;
+    OPE_CHECK(cudaEventCreate(&e0));
+    OPE_CHECK(cudaEventCreate(&e1));
+    k_dfma_probe<<<blocks, threads, 0, c.stream>>>(0.999999, 1e-7, 20000, static_cast<double*>(ws));
+    OPE_CHECK(cudaGetLastError());
+    const int iters = 400000;
+    OPE_CHECK(cudaEventRecord(e0, c.stream));
+    k_dfma_probe<<<blocks, threads, 0, c.stream>>>(0.999999, 1e-7, iters, static_cast<double*>(ws));
+    OPE_CHECK(cudaGetLastError());
+    OPE_CHECK(cudaEventRecord(e1, c.stream));
+    OPE_CHECK(cudaEventSynchronize(e1));
+    float t = 0.f;
+    OPE_CHECK(cudaEventElapsedTime(&t, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c.launches += 2;
+    *ms = t;
+    *flops = 2.0 * 8.0 * (double)iters * (double)threads * (double)blocks / (t * 1e-3);
+    return OPE_OK;
+}
+
+}  // namespace ope

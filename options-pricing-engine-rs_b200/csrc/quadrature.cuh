@@ -1,0 +1,193 @@
+// Warp-cooperative greedy globally-adaptive Gauss-Kronrod-15 on [0, 1].
+//
+// Reference: heston.rs:180-212 (gk15_panel, adaptive_gk), heston.rs:29-59
+// (nodes/weights), heston.rs:220-229 (gk_integrate).
+//
+// One warp integrates one integral.  Each step bisects the live panel with
+// the largest error estimate: lanes 0-14 evaluate the 15 Kronrod nodes of the
+// left child and lanes 16-30 those of the right child (30 of 32 lanes busy);
+// half-warp shuffle trees reduce the K15 and G7 sums.  The live-panel list
+// (at most 200 entries of {err, K, a, b}) sits in shared memory, one list per
+// warp, and is maintained exactly as the reference maintains its Vec:
+//   * argmax by f64::total_cmp with the LAST maximum winning ties (errors are
+//     non-negative, so their IEEE bit patterns compare as unsigned integers
+//     in total_cmp order, and the comparison uses the integer pipe);
+//   * swap_remove of the chosen panel, then push(left), push(right);
+//   * total += kl + kr - kw; err += el + er - ew, in that association;
+//   * stop when err <= tol or 200 panels are live.
+// Node positions c + h*x_i and the panel products K*h, |K-G|*h are rounded
+// exactly as the reference rounds them (no FMA contraction), so the panel
+// geometry is bit-identical; only the integrand values and the order of the
+// 15-term sums differ at the last-ulp level.
+#pragma once
+
+#include "cf_device.cuh"
+
+namespace ope {
+
+constexpr int kMaxPanels = 200;  // heston.rs:194
+
+// GK15 nodes and weights in the reference's order (heston.rs:29-49) with a
+// zero pad at index 15, and the G7 weight scattered onto its Kronrod index
+// (G7_IDX = {0,3,4,7,8,11,12}, heston.rs:53-59), zero elsewhere.
+__constant__ double c_gk_x[16] = {
+    0.0,
+    0.2077849550078985, -0.2077849550078985,
+    0.4058451513773972, -0.4058451513773972,
+    0.5860872354676911, -0.5860872354676911,
+    0.7415311855993945, -0.7415311855993945,
+    0.8648644233597691, -0.8648644233597691,
+    0.9491079123427585, -0.9491079123427585,
+    0.9914553711208126, -0.9914553711208126,
+    0.0};
+__constant__ double c_gk_wk[16] = {
+    0.2094821410847278,
+    0.2044329400752989, 0.2044329400752989,
+    0.1903505780647854, 0.1903505780647854,
+    0.1690047266392679, 0.1690047266392679,
+    0.1406532597155259, 0.1406532597155259,
+    0.1047900103222502, 0.1047900103222502,
+    0.0630920926299786, 0.0630920926299786,
+    0.0229353220105292, 0.0229353220105292,
+    0.0};
+__constant__ double c_gk_wg[16] = {
+    0.4179591836734694,
+    0.0, 0.0,
+    0.3818300505051189, 0.3818300505051189,
+    0.0, 0.0,
+    0.2797053914892766, 0.2797053914892766,
+    0.0, 0.0,
+    0.1294849661688697, 0.1294849661688697,
+    0.0, 0.0,
+    0.0};
+
+// One warp's live-panel list (structure of arrays, 6400 bytes).
+struct PanelStore {
+    unsigned long long ekey[kMaxPanels];  // error as IEEE bits (total_cmp order for err >= 0)
+    double k[kMaxPanels];
+    double a[kMaxPanels];
+    double b[kMaxPanels];
+};
+
+// Per-lane quadrature constants, loaded once per warp.
+struct LaneRule {
+    double x, wk, wg;
+    bool node;  // lane holds a Kronrod node (lane % 16 < 15)
+    int half;   // 0 = left child, 1 = right child
+};
+
+__device__ __forceinline__ LaneRule lane_rule(int lane) {
+    LaneRule R;
+    const int j = lane & 15;
+    R.x = c_gk_x[j];
+    R.wk = c_gk_wk[j];
+    R.wg = c_gk_wg[j];
+    R.node = j < 15;
+    R.half = lane >> 4;
+    return R;
+}
+
+__device__ __forceinline__ void half_warp_sum2(double& a, double& b) {
+#pragma unroll
+    for (int off = 8; off > 0; off >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, off);
+        b += __shfl_xor_sync(0xffffffffu, b, off);
+    }
+}
+
+// Returns the integral (identical in every lane).  `nbis` receives the
+// number of bisections (loop iterations of heston.rs:200-210).
+template <bool BATES>
+__device__ __forceinline__ double gk_integrate_warp(const CfConsts& C, double tol, PanelStore& L, int lane,
+                                                    const LaneRule& R, int* nbis) {
+    const unsigned FULL = 0xffffffffu;
+    // First panel [0, 1]: c = h = 0.5; only the left half-warp has nodes.
+    double f = 0.0;
+    if (R.half == 0 && R.node) f = node_value<BATES>(C, __dadd_rn(0.5, __dmul_rn(0.5, R.x)));
+    double ks = R.wk * f, gs = R.wg * f;
+    half_warp_sum2(ks, gs);
+    const double K0 = __shfl_sync(FULL, ks, 0), G0 = __shfl_sync(FULL, gs, 0);
+    const double k0 = __dmul_rn(K0, 0.5);
+    const double e0 = __dmul_rn(fabs(K0 - G0), 0.5);
+    if (lane == 0) {
+        L.ekey[0] = (unsigned long long)__double_as_longlong(e0);
+        L.k[0] = k0;
+        L.a[0] = 0.0;
+        L.b[0] = 1.0;
+    }
+    __syncwarp();
+    double total = k0, err = e0;
+    int len = 1, nb = 0;
+    while (err > tol && len < kMaxPanels) {
+        // argmax over the live list, last maximum wins (Iterator::max_by).
+        unsigned long long best = 0ull;
+        int bi = -1;
+        for (int i = lane; i < len; i += 32) {
+            const unsigned long long kk = L.ekey[i];
+            if (kk >= best) { best = kk; bi = i; }
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            const unsigned long long ob = __shfl_xor_sync(FULL, best, off);
+            const int oi = __shfl_xor_sync(FULL, bi, off);
+            if (ob > best || (ob == best && oi > bi)) { best = ob; bi = oi; }
+        }
+        const int w = bi;
+        const double ew = __longlong_as_double((long long)best);
+        const double kw = L.k[w], aw = L.a[w], bw = L.b[w];
+        const double m = 0.5 * (aw + bw);
+        const double pa = R.half ? m : aw, pb = R.half ? bw : m;
+        const double c = 0.5 * (pa + pb), h = 0.5 * (pb - pa);
+        f = R.node ? node_value<BATES>(C, __dadd_rn(c, __dmul_rn(h, R.x))) : 0.0;
+        ks = R.wk * f;
+        gs = R.wg * f;
+        half_warp_sum2(ks, gs);
+        const double Kl = __shfl_sync(FULL, ks, 0), Gl = __shfl_sync(FULL, gs, 0);
+        const double Kr = __shfl_sync(FULL, ks, 16), Gr = __shfl_sync(FULL, gs, 16);
+        const double hl = 0.5 * (m - aw), hr = 0.5 * (bw - m);
+        const double kl = __dmul_rn(Kl, hl), el = __dmul_rn(fabs(Kl - Gl), hl);
+        const double kr = __dmul_rn(Kr, hr), er = __dmul_rn(fabs(Kr - Gr), hr);
+        total = __dadd_rn(total, __dsub_rn(__dadd_rn(kl, kr), kw));
+        err = __dadd_rn(err, __dsub_rn(__dadd_rn(el, er), ew));
+        __syncwarp();  // every lane has read entry w
+        if (lane == 0) {
+            const int last = len - 1;
+            if (w != last) {  // swap_remove
+                L.ekey[w] = L.ekey[last];
+                L.k[w] = L.k[last];
+                L.a[w] = L.a[last];
+                L.b[w] = L.b[last];
+            }
+            L.ekey[last] = (unsigned long long)__double_as_longlong(el);
+            L.k[last] = kl;
+            L.a[last] = aw;
+            L.b[last] = m;
+            L.ekey[len] = (unsigned long long)__double_as_longlong(er);
+            L.k[len] = kr;
+            L.a[len] = m;
+            L.b[len] = bw;
+        }
+        __syncwarp();
+        ++len;
+        ++nb;
+    }
+    *nbis = nb;
+    return total;
+}
+
+// heston.rs:95-98 + heston.rs:70 (bates.rs:60-62, 37): the Gil-Pelaez
+// combination, the max(.,0) clamp on the call, put by parity.  Rounded in the
+// reference's association order (no FMA).
+__device__ __forceinline__ double finish_price(double s, double k, double t, double r, double q, int opt_type,
+                                               double i1, double i2) {
+    const double PI = 3.14159265358979323846;
+    const double p1 = __dadd_rn(0.5, i1 / PI);
+    const double p2 = __dadd_rn(0.5, i2 / PI);
+    const double seq = __dmul_rn(s, exp(-q * t));
+    const double ker = __dmul_rn(k, exp(-r * t));
+    const double call = fmax(__dsub_rn(__dmul_rn(seq, p1), __dmul_rn(ker, p2)), 0.0);
+    if (opt_type == 0) return call;
+    return __dadd_rn(__dsub_rn(call, seq), ker);
+}
+
+}  // namespace ope

@@ -1,0 +1,250 @@
+"""Host-side mirror of the reference crate's pricing API over the C ABI.
+
+Names, argument order and meaning follow the reference's public surface
+(lib.rs:18-35): ``heston_price`` / ``bates_price`` (heston.rs:61, bates.rs:29),
+``batch_heston`` / ``batch_bates`` / ``batch_heston_greeks`` /
+``batch_bates_greeks`` (batch.rs:23-48) and the records ``OptionType``,
+``OptionContract``, ``PricingResult``, ``HestonParams``, ``BatesParams``
+(types.rs).  Where the reference panics this raises ``OpeError``; there is no
+CPU fallback.  The quadrature tolerance defaults to the reference's 1e-8
+(heston.rs:228); every entry point also takes ``tol=``.
+
+Beyond the reference: ``price_surfaces`` (many surfaces, one persistent
+launch) and ``*_device`` variants that take torch CUDA tensors already
+resident in HBM and run stream-ordered on the current torch stream.
+"""
+from __future__ import annotations
+
+import ctypes
+import enum
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from ._lib import MODEL_BATES, MODEL_HESTON, OpeError, Options, check, load
+from .workloads import CONTRACT_DTYPE
+
+REF_TOL = 1e-8
+
+RESULT_DTYPE = np.dtype([(k, "<f8") for k in ("price", "delta", "gamma", "vega", "theta", "rho", "vanna", "volga")])
+
+
+class OptionType(enum.IntEnum):  # types.rs:5-13
+    Call = 0
+    Put = 1
+
+    def sign(self) -> float:
+        return 1.0 if self == OptionType.Call else -1.0
+
+
+@dataclass
+class OptionContract:  # types.rs:16-25
+    spot: float
+    strike: float
+    expiry: float
+    rate: float
+    div_yield: float
+    vol: float
+    opt_type: OptionType = OptionType.Call
+
+
+@dataclass
+class HestonParams:  # types.rs:48-63
+    v0: float
+    kappa: float
+    theta: float
+    sigma: float
+    rho: float
+
+    def feller_ok(self) -> bool:
+        return 2.0 * self.kappa * self.theta > self.sigma * self.sigma
+
+    def as_array(self) -> np.ndarray:
+        return np.array([self.v0, self.kappa, self.theta, self.sigma, self.rho], dtype=np.float64)
+
+
+@dataclass
+class BatesParams:  # types.rs:66-72
+    heston: HestonParams
+    lambda_: float
+    mu_j: float
+    sigma_j: float
+
+    def as_array(self) -> np.ndarray:
+        return np.concatenate([self.heston.as_array(), [self.lambda_, self.mu_j, self.sigma_j]]).astype(np.float64)
+
+
+@dataclass
+class PricingResult:  # types.rs:29-39
+    price: float = 0.0
+    delta: float = 0.0
+    gamma: float = 0.0
+    vega: float = 0.0
+    theta: float = 0.0
+    rho: float = 0.0
+    vanna: float = 0.0
+    volga: float = 0.0
+
+
+def _params_array(params, model: int) -> np.ndarray:
+    if isinstance(params, (HestonParams, BatesParams)):
+        arr = params.as_array()
+    else:
+        arr = np.ascontiguousarray(params, dtype=np.float64)
+    want = 8 if model == MODEL_BATES else 5
+    if arr.shape[-1] != want:
+        raise ValueError(f"expected {want} parameters per set, got shape {arr.shape}")
+    return np.ascontiguousarray(arr, dtype=np.float64)
+
+
+def contracts_array(contracts) -> np.ndarray:
+    """OptionContract list / structured array -> contiguous ope_contract records."""
+    if isinstance(contracts, np.ndarray) and contracts.dtype == CONTRACT_DTYPE:
+        return np.ascontiguousarray(contracts)
+    out = np.zeros(len(contracts), CONTRACT_DTYPE)
+    for i, c in enumerate(contracts):
+        out[i] = (c.spot, c.strike, c.expiry, c.rate, c.div_yield, c.vol, int(c.opt_type), 0)
+    return out
+
+
+def _opts(tol: float, flags: int = 0, stream: int = 0) -> Options:
+    return Options(tol=float(tol), flags=flags, reserved=0, stream=stream or None)
+
+
+def heston_price(spot, strike, expiry, rate, div_yield, params, opt_type=OptionType.Call, tol=REF_TOL) -> float:
+    """heston.rs:61-72."""
+    return float(batch_heston([OptionContract(spot, strike, expiry, rate, div_yield, 0.0, OptionType(opt_type))],
+                              params, tol=tol)[0])
+
+
+def bates_price(spot, strike, expiry, rate, div_yield, params, opt_type=OptionType.Call, tol=REF_TOL) -> float:
+    """bates.rs:29-39."""
+    return float(batch_bates([OptionContract(spot, strike, expiry, rate, div_yield, 0.0, OptionType(opt_type))],
+                             params, tol=tol)[0])
+
+
+def _batch(model: int, contracts, params, tol: float) -> np.ndarray:
+    con = contracts_array(contracts)
+    p = _params_array(params, model)
+    out = np.empty(con.size, dtype=np.float64)
+    if con.size == 0:
+        return out
+    o = _opts(tol)
+    check(load().ope_batch_price_ex(model, con.ctypes.data, con.size, p.ctypes.data, out.ctypes.data,
+                                    ctypes.byref(o)))
+    return out
+
+
+def batch_heston(contracts, params, tol=REF_TOL) -> np.ndarray:
+    """batch.rs:23-27 — one parameter set, prices in input order."""
+    return _batch(MODEL_HESTON, contracts, params, tol)
+
+
+def batch_bates(contracts, params, tol=REF_TOL) -> np.ndarray:
+    """batch.rs:38-42."""
+    return _batch(MODEL_BATES, contracts, params, tol)
+
+
+def _batch_greeks(model: int, contracts, params, tol: float) -> np.ndarray:
+    con = contracts_array(contracts)
+    p = _params_array(params, model)
+    out = np.zeros(con.size, dtype=RESULT_DTYPE)
+    if con.size == 0:
+        return out
+    if tol == REF_TOL:
+        fn = load().ope_batch_bates_greeks if model == MODEL_BATES else load().ope_batch_heston_greeks
+        check(fn(con.ctypes.data, con.size, p.ctypes.data, out.ctypes.data))
+    else:
+        o = _opts(tol)
+        check(load().ope_batch_greeks_ex(model, con.ctypes.data, con.size, p.ctypes.data, out.ctypes.data,
+                                         ctypes.byref(o)))
+    return out
+
+
+def batch_heston_greeks(contracts, params, tol=REF_TOL) -> np.ndarray:
+    """batch.rs:32-36 (bump-and-reprice, greeks.rs:19-72).  Structured array of PricingResult."""
+    return _batch_greeks(MODEL_HESTON, contracts, params, tol)
+
+
+def batch_bates_greeks(contracts, params, tol=REF_TOL) -> np.ndarray:
+    """batch.rs:44-48."""
+    return _batch_greeks(MODEL_BATES, contracts, params, tol)
+
+
+def price_surfaces(model: int, contracts, surf_offsets, params, tol=REF_TOL, out=None,
+                   bisections=None) -> np.ndarray:
+    """Many surfaces (one parameter set each) in ONE persistent launch.
+
+    ``out`` (float64, n) may be a caller-owned (e.g. pinned) buffer; with
+    ``bisections`` (int32, 2n) the per-integral bisection counts are returned too.
+    """
+    con = contracts_array(contracts)
+    off = np.ascontiguousarray(surf_offsets, dtype=np.int64)
+    p = _params_array(params, model)
+    n_surf = off.size - 1
+    if p.ndim != 2 or p.shape[0] != n_surf:
+        raise ValueError("params must be (n_surf, 5|8)")
+    if out is None:
+        out = np.empty(con.size, dtype=np.float64)
+    if con.size == 0:
+        return out
+    o = _opts(tol)
+    if bisections is None:
+        check(load().ope_price_surfaces(model, con.ctypes.data, con.size, off.ctypes.data, n_surf, p.ctypes.data,
+                                        out.ctypes.data, ctypes.byref(o)))
+    else:
+        assert bisections.dtype == np.int32 and bisections.size == 2 * con.size
+        check(load().ope_price_surfaces_stats(model, con.ctypes.data, con.size, off.ctypes.data, n_surf,
+                                              p.ctypes.data, out.ctypes.data, bisections.ctypes.data,
+                                              ctypes.byref(o)))
+    return out
+
+
+def measure_fp64_peak() -> tuple[float, float]:
+    """(flop/s, ms) of the DFMA throughput probe on the current device."""
+    f, ms = ctypes.c_double(), ctypes.c_double()
+    check(load().ope_measure_fp64_peak(ctypes.byref(f), ctypes.byref(ms)))
+    return f.value, ms.value
+
+
+# ---------------------------------------------------------------- device path
+def _torch_stream_ptr() -> int:
+    import torch
+
+    return torch.cuda.current_stream().cuda_stream
+
+
+def price_surfaces_device(model: int, d_contracts, n: int, d_offsets, n_surf: int, d_params, d_out,
+                          tol=REF_TOL, stream: int | None = None) -> None:
+    """Stream-ordered persistent launch over device buffers (torch tensors or raw pointers)."""
+    ptr = lambda t: t if isinstance(t, int) else t.data_ptr()  # noqa: E731
+    o = _opts(tol, _lib.FLAG_DEVICE_PTRS, _torch_stream_ptr() if stream is None else stream)
+    check(load().ope_price_surfaces(model, ptr(d_contracts), n, ptr(d_offsets), n_surf, ptr(d_params), ptr(d_out),
+                                    ctypes.byref(o)))
+
+
+def batch_price_device(model: int, d_contracts, n: int, d_params, d_out, tol=REF_TOL,
+                       stream: int | None = None) -> None:
+    """Stream-ordered plain (single parameter set) launch over device buffers."""
+    ptr = lambda t: t if isinstance(t, int) else t.data_ptr()  # noqa: E731
+    o = _opts(tol, _lib.FLAG_DEVICE_PTRS, _torch_stream_ptr() if stream is None else stream)
+    check(load().ope_batch_price_ex(model, ptr(d_contracts), n, ptr(d_params), ptr(d_out), ctypes.byref(o)))
+
+
+def kernel_launch_count() -> int:
+    return int(load().ope_kernel_launch_count())
+
+
+def device_info() -> tuple[int, int, int]:
+    sm, ma, mi = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+    check(load().ope_device_info(ctypes.byref(sm), ctypes.byref(ma), ctypes.byref(mi)))
+    return sm.value, ma.value, mi.value
+
+
+__all__ = [
+    "OptionType", "OptionContract", "HestonParams", "BatesParams", "PricingResult", "OpeError",
+    "heston_price", "bates_price", "batch_heston", "batch_bates", "batch_heston_greeks", "batch_bates_greeks",
+    "price_surfaces", "price_surfaces_device", "batch_price_device", "contracts_array", "REF_TOL",
+    "MODEL_HESTON", "MODEL_BATES", "RESULT_DTYPE", "kernel_launch_count", "device_info", "measure_fp64_peak",
+]

@@ -1,0 +1,264 @@
+"""GPU parity: the CUDA path (through the C ABI) against the CPU oracle.
+
+Tolerance (the pricing path's contract): |price_gpu - price_oracle| <= 1e-9 * S
+per contract, at the same quadrature tolerance.  The reference's own test
+invariants (heston.rs:309-427, bates.rs:98-173, batch.rs:270-319) are re-run
+on the GPU path with the reference's tolerances.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from ope_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+S = 100.0
+PRICE_TOL = 1e-9 * S
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+H_REF = [0.04, 2.0, 0.04, 0.3, -0.7]  # heston.rs:236-239
+B_REF = H_REF + [0.5, -0.1, 0.15]     # bates.rs:94-96
+
+
+def _max_err(a, b):
+    return float(np.max(np.abs(np.asarray(a) - np.asarray(b)))) if np.size(a) else 0.0
+
+
+def test_c1_plain_matches_oracle(ope, oracle):
+    w = W.c1()
+    got = ope.batch_heston(w.contracts, w.params[0], tol=w.tol)
+    ref = oracle.batch_price(w.contracts, w.params, False, w.tol)
+    assert _max_err(got, ref) <= PRICE_TOL
+    with open(os.path.join(HERE, "golden", "oracle_c1.json")) as f:
+        gold = np.array([float.fromhex(h) for h in json.load(f)["price"]])
+    assert _max_err(got, gold) <= PRICE_TOL
+
+
+def test_c1_reference_tolerance_matches_oracle(ope, oracle):
+    w = W.c1()
+    got = ope.batch_heston(w.contracts, w.params[0])  # tol = 1e-8, the reference's
+    ref = oracle.batch_price(w.contracts, w.params, False, 1e-8)
+    assert _max_err(got, ref) <= PRICE_TOL
+
+
+def test_persistent_equals_plain_bitwise(ope):
+    w = W.c1()
+    plain = ope.batch_heston(w.contracts, w.params[0], tol=w.tol)
+    pers = ope.price_surfaces(ope.MODEL_HESTON, w.contracts, w.surf_offsets, w.params, tol=w.tol)
+    assert np.array_equal(plain.view(np.uint64), pers.view(np.uint64))
+
+
+def test_c2_sample_matches_oracle(ope, oracle):
+    w = W.c2()
+    rng = np.random.default_rng(11)
+    sub = w.subset(np.sort(rng.choice(w.n_surf, 48, replace=False)))
+    got = ope.price_surfaces(ope.MODEL_HESTON, sub.contracts, sub.surf_offsets, sub.params, tol=sub.tol)
+    ref = oracle.batch_price(sub.contracts, sub.params, False, sub.tol, surf_idx=sub.surf_idx())
+    err = np.abs(got - ref)
+    assert float(err.max()) <= PRICE_TOL, f"worst contract {int(err.argmax())}: {err.max():.3e}"
+
+
+def test_c3_sample_matches_oracle(ope, oracle):
+    w = W.c3()
+    rng = np.random.default_rng(12)
+    sub = w.subset(np.sort(rng.choice(w.n_surf, 48, replace=False)))
+    got = ope.price_surfaces(ope.MODEL_BATES, sub.contracts, sub.surf_offsets, sub.params, tol=sub.tol)
+    ref, nb = oracle.batch_price(sub.contracts, sub.params, True, sub.tol, surf_idx=sub.surf_idx(), stats=True)
+    err = np.abs(got - ref)
+    assert float(err.max()) <= PRICE_TOL, f"worst contract {int(err.argmax())}: {err.max():.3e}"
+
+
+def test_capped_integrals_match_oracle(ope, oracle):
+    """Contracts whose integrals stop at the 200-panel cap (heston.rs:194)."""
+    w = W.c3(n=1 << 16)
+    ref, nb = oracle.batch_price(w.contracts, w.params, True, w.tol, surf_idx=w.surf_idx(), stats=True)
+    capped = np.where(nb.reshape(-1, 2).max(axis=1) >= 199)[0]
+    assert capped.size > 0
+    got = ope.price_surfaces(ope.MODEL_BATES, w.contracts, w.surf_offsets, w.params, tol=w.tol)
+    assert _max_err(got[capped], ref[capped]) <= PRICE_TOL
+    assert _max_err(got, ref) <= PRICE_TOL
+
+
+def test_bates_plain_matches_oracle_all_types(ope, oracle):
+    con = oracle.contracts(100.0, np.repeat([70.0, 90.0, 100.0, 110.0, 150.0], 4),
+                           np.tile([1 / 365, 0.05, 1.0, 3.0], 5), 0.03, 0.01, np.arange(20) % 2)
+    got = ope.batch_bates(con, B_REF, tol=1e-10)
+    ref = oracle.batch_price(con, np.array([B_REF]), True, 1e-10)
+    assert _max_err(got, ref) <= PRICE_TOL
+
+
+# --- the reference's own invariants, on the GPU path -----------------------
+
+def test_put_call_parity_heston(ope):  # heston.rs:309-316
+    call = ope.heston_price(100.0, 100.0, 0.5, 0.03, 0.0, H_REF, 0)
+    put = ope.heston_price(100.0, 100.0, 0.5, 0.03, 0.0, H_REF, 1)
+    er = np.exp(-0.03 * 0.5)
+    assert abs(call - put - (100.0 - 100.0 * er)) < 0.01
+
+
+def test_price_sanity(ope):  # heston.rs:318-327
+    call = ope.heston_price(100.0, 100.0, 1.0, 0.05, 0.0, H_REF, 0)
+    put = ope.heston_price(100.0, 100.0, 1.0, 0.05, 0.0, H_REF, 1)
+    assert abs(call - put - 100.0 + 100.0 * np.exp(-0.05)) < 0.05
+    assert call >= 0.0
+
+
+@pytest.mark.parametrize("bates", [False, True])
+def test_no_static_arbitrage(ope, bates):  # heston.rs:382-406, bates.rs:147-173
+    sets = ([[0.04, 2.0, 0.04, 0.3, -0.7, 0.5, -0.1, 0.15], [0.09, 1.0, 0.09, 0.8, -0.5, 1.0, -0.2, 0.25]]
+            if bates else [[0.04, 2.0, 0.04, 0.3, -0.7], [0.09, 1.0, 0.09, 0.8, -0.5], [0.04, 0.5, 0.04, 0.5, -0.7]])
+    s, r, q = 100.0, 0.03, 0.0
+    expiries = [0.02, 0.1, 0.25, 0.5, 1.0, 2.0]
+    strikes = [70.0, 85.0, 100.0, 115.0, 130.0, 150.0, 200.0]
+    for p in sets:
+        con = np.zeros(len(expiries) * len(strikes), W.CONTRACT_DTYPE)
+        TT, KK = np.meshgrid(expiries, strikes, indexing="ij")
+        con["spot"], con["strike"], con["expiry"], con["rate"], con["div_yield"] = s, KK.ravel(), TT.ravel(), r, q
+        px = (ope.batch_bates if bates else ope.batch_heston)(con, p).reshape(len(expiries), len(strikes))
+        for i, t in enumerate(expiries):
+            cap = s * np.exp(-q * t)
+            prev = np.inf
+            for j, k in enumerate(strikes):
+                c = px[i, j]
+                intrinsic = max(s * np.exp(-q * t) - k * np.exp(-r * t), 0.0)
+                assert c >= intrinsic - 1e-4 and c <= cap + 1e-4 and c <= prev + 1e-4, (p, t, k, c)
+                prev = c
+
+
+def test_zero_vol_of_vol_matches_bsm(ope, oracle):  # heston.rs:411-427
+    p = [0.04, 1.0, 0.04, 1e-4, 0.0]
+    for t in (0.25, 1.0, 2.0):
+        for k in (70.0, 85.0, 100.0, 115.0, 130.0):
+            h = ope.heston_price(100.0, k, t, 0.03, 0.0, p, 0)
+            b = oracle.bsm_price(oracle.contracts(100.0, k, t, 0.03, 0.0, 0, vol=0.2))
+            assert abs(h - b) < 0.02
+
+
+def test_bates_recovers_heston_no_jumps(ope):  # bates.rs:98-106
+    b = ope.bates_price(100.0, 100.0, 1.0, 0.05, 0.0, H_REF + [0.0, 0.0, 1e-8], 0)
+    h = ope.heston_price(100.0, 100.0, 1.0, 0.05, 0.0, H_REF, 0)
+    assert abs(b - h) < 0.02
+
+
+def test_put_call_parity_bates(ope):  # bates.rs:108-115
+    call = ope.bates_price(100.0, 100.0, 0.5, 0.03, 0.0, B_REF, 0)
+    put = ope.bates_price(100.0, 100.0, 0.5, 0.03, 0.0, B_REF, 1)
+    assert abs(call - put - (100.0 - 100.0 * np.exp(-0.03 * 0.5))) < 0.02
+
+
+def _chain(n):  # batch.rs:238-244
+    c = np.zeros(n, W.CONTRACT_DTYPE)
+    c["spot"], c["strike"], c["expiry"], c["rate"], c["div_yield"], c["vol"] = 100.0, 80.0 + 2.0 * np.arange(n), 0.5, 0.03, 0.0, 0.2
+    return c
+
+
+@pytest.mark.parametrize("bates", [False, True])
+def test_batch_greeks_match_oracle(ope, oracle, bates):  # batch.rs:270-306 against the oracle
+    c = _chain(15)
+    p = B_REF if bates else H_REF
+    fn = ope.batch_bates_greeks if bates else ope.batch_heston_greeks
+    got = fn(c, p, tol=1e-10)
+    ref = oracle.batch_greeks(c, p, bates, tol=1e-10)
+    names = ["price", "delta", "gamma", "vega", "theta", "rho", "vanna", "volga"]
+    # finite-difference amplification of a 1e-9*S price tolerance per greek
+    amp = {"price": 1, "delta": 1, "gamma": 4, "vega": 100, "theta": 2 * 365, "rho": 1e4, "vanna": 200,
+           "volga": 2e4}
+    for i, nm in enumerate(names):
+        err = _max_err(got[nm], ref[:, i])
+        assert err <= PRICE_TOL * amp[nm], (nm, err)
+    # batch price == batch greeks price (batch.rs:310-319)
+    px = (ope.batch_bates if bates else ope.batch_heston)(c, p, tol=1e-10)
+    assert np.array_equal(px, got["price"])
+
+
+def test_greeks_signs_reference_tolerance(ope):  # heston.rs:334-350
+    c = _chain(1)
+    c["strike"], c["expiry"], c["rate"] = 100.0, 1.0, 0.05
+    r = ope.batch_heston_greeks(c, H_REF)[0]
+    assert 0.0 < r["delta"] < 1.0 and r["gamma"] > 0 and r["vega"] > 0 and r["rho"] > 0
+    c["opt_type"] = 1
+    r = ope.batch_heston_greeks(c, H_REF)[0]
+    assert -1.0 < r["delta"] < 0.0 and r["gamma"] > 0
+
+
+# --- edge cases ---------------------------------------------------------------
+
+def test_empty_and_single(ope, oracle):
+    assert ope.batch_heston(np.zeros(0, W.CONTRACT_DTYPE), H_REF).size == 0
+    assert ope.price_surfaces(ope.MODEL_BATES, np.zeros(0, W.CONTRACT_DTYPE), [0], [B_REF]).size == 0
+    v = ope.bates_price(100.0, 120.0, 1 / 365, 0.03, 0.01, B_REF, 1, tol=1e-10)
+    r = oracle.bates_price(100.0, 120.0, 1 / 365, 0.03, 0.01, B_REF, 1, 1e-10)
+    assert abs(v - r) <= PRICE_TOL
+
+
+def test_ragged_surfaces_and_empty_surfaces(ope, oracle):
+    w = W.c2(n_surf=24, seed=5)
+    counts = np.diff(w.surf_offsets)
+    counts[3] = 0
+    counts[7] = 0
+    keep = np.concatenate([np.arange(w.surf_offsets[s], w.surf_offsets[s] + counts[s]) for s in range(24)])
+    con = w.contracts[keep]
+    off = np.concatenate([[0], np.cumsum(counts)])
+    got = ope.price_surfaces(ope.MODEL_HESTON, con, off, w.params, tol=w.tol)
+    ref = oracle.batch_price(con, w.params, False, w.tol, surf_idx=np.repeat(np.arange(24), counts).astype(np.int32))
+    assert _max_err(got, ref) <= PRICE_TOL
+
+
+def test_nan_parameters_stay_in_their_surface(ope, oracle):
+    w = W.c3(n=2048, per_surface=256)
+    params = w.params.copy()
+    params[2, 1] = np.nan
+    got = ope.price_surfaces(ope.MODEL_BATES, w.contracts, w.surf_offsets, params, tol=w.tol)
+    ref = oracle.batch_price(w.contracts, params, True, w.tol, surf_idx=w.surf_idx())
+    s2 = slice(w.surf_offsets[2], w.surf_offsets[3])
+    mask = np.ones(w.n, bool)
+    mask[s2] = False
+    assert _max_err(got[mask], ref[mask]) <= PRICE_TOL
+    # inside the poisoned surface the GPU must behave like the reference (NaN in, same out)
+    assert np.array_equal(np.isnan(got[s2]), np.isnan(ref[s2]))
+    fin = ~np.isnan(ref[s2])
+    assert _max_err(got[s2][fin], ref[s2][fin]) <= PRICE_TOL
+
+
+def test_invalid_arguments_are_rejected(ope):
+    import ctypes
+
+    from ope_b200 import _lib
+
+    L = _lib.load()
+    out = np.zeros(4)
+    assert L.ope_batch_heston(None, 4, None, out.ctypes.data) == 1
+    con = _chain(4)
+    off_bad = np.array([0, 3, 2], np.int64)
+    p = np.array([H_REF, H_REF])
+    rc = L.ope_price_surfaces(0, con.ctypes.data, 4, off_bad.ctypes.data, 2, p.ctypes.data, out.ctypes.data, None)
+    assert rc == 1
+    o = _lib.Options(tol=float("nan"), flags=0, reserved=0, stream=None)
+    rc = L.ope_batch_price_ex(0, con.ctypes.data, 4, p.ctypes.data, out.ctypes.data, ctypes.byref(o))
+    assert rc == 1
+    assert L.ope_batch_price_ex(7, con.ctypes.data, 4, p.ctypes.data, out.ctypes.data, None) == 1
+
+
+# --- full-size properties (no oracle at this size) ---------------------------
+
+def test_full_c3_properties_and_determinism(ope):
+    w = W.c3()
+    a = ope.price_surfaces(ope.MODEL_BATES, w.contracts, w.surf_offsets, w.params, tol=w.tol)
+    b = ope.price_surfaces(ope.MODEL_BATES, w.contracts, w.surf_offsets, w.params, tol=w.tol)
+    assert np.array_equal(a.view(np.uint64), b.view(np.uint64)), "run-to-run determinism"
+    assert np.all(np.isfinite(a))
+    c = w.contracts
+    eq, er = np.exp(-c["div_yield"] * c["expiry"]), np.exp(-c["rate"] * c["expiry"])
+    fwd_call_lb = np.maximum(c["spot"] * eq - c["strike"] * er, 0.0)
+    fwd_put_lb = np.maximum(c["strike"] * er - c["spot"] * eq, 0.0)
+    lb = np.where(c["opt_type"] == 0, fwd_call_lb, fwd_put_lb)
+    ub = np.where(c["opt_type"] == 0, c["spot"] * eq, c["strike"] * er)
+    assert np.all(a >= lb - 1e-4) and np.all(a <= ub + 1e-4)
+    # one surface alone gives the same bits as inside the full batch
+    s = 1234
+    sub = w.subset([s])
+    alone = ope.price_surfaces(ope.MODEL_BATES, sub.contracts, sub.surf_offsets, sub.params, tol=w.tol)
+    assert np.array_equal(alone, a[w.surf_offsets[s]:w.surf_offsets[s + 1]])
