@@ -125,8 +125,8 @@ int batch_price(int32_t model, const ope_contract* contracts, size_t n, const vo
     if (device_ptrs(opts)) {
         void* ws;
         OPE_TRY(ensure_workspace(price_scratch_bytes(n), &ws));
-        return launch_price_plain(model, contracts, n, static_cast<const double*>(params), tol, out,
-                                  carve_price_scratch(ws, n), user_stream(opts));
+        return launch_price_persistent(model, contracts, n, nullptr, 1, nullptr, static_cast<const double*>(params),
+                                       tol, out, carve_price_scratch(ws, n), user_stream(opts));
     }
     ThreadCtx& c = tctx();
     const size_t b_con = align_up(n * sizeof(ope_contract), 256), b_par = 256, b_out = align_up(n * sizeof(double), 256);
@@ -139,7 +139,8 @@ int batch_price(int32_t model, const ope_contract* contracts, size_t n, const vo
     void* scratch = p + b_con + b_par + b_out;
     OPE_CHECK(cudaMemcpyAsync(d_con, contracts, n * sizeof(ope_contract), cudaMemcpyHostToDevice, c.stream));
     OPE_CHECK(cudaMemcpyAsync(d_par, params, stride * sizeof(double), cudaMemcpyHostToDevice, c.stream));
-    OPE_TRY(launch_price_plain(model, d_con, n, d_par, tol, d_out, carve_price_scratch(scratch, n), c.stream));
+    OPE_TRY(launch_price_persistent(model, d_con, n, nullptr, 1, nullptr, d_par, tol, d_out,
+                                    carve_price_scratch(scratch, n), c.stream));
     OPE_CHECK(cudaMemcpyAsync(out, d_out, n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
     OPE_CHECK(cudaStreamSynchronize(c.stream));
     return OPE_OK;

@@ -60,8 +60,6 @@ size_t price_scratch_bytes(size_t n);
 PriceScratch carve_price_scratch(void* base, size_t n);
 
 // Device launchers (stream-ordered; all pointers are device pointers).
-int launch_price_plain(int model, const ope_contract* con, size_t n, const double* params, double tol,
-                       double* out, const PriceScratch& s, cudaStream_t st, int32_t* nbis_out = nullptr);
 // Contract c is priced with params + stride * p(c), where p(c) = param_idx[c]
 // when param_idx is non-NULL, else the surface of c under surf_offsets
 // (n_surf + 1 entries), else 0.

@@ -1,5 +1,8 @@
-// Pricing kernels: the plain per-surface launch (batch.rs:23-42 drop-in) and
-// the persistent multi-surface launch with a device work queue.
+// The pricing kernel: a persistent grid of warps pulling (contract, integral)
+// units from a device work queue.  The same kernel serves the plain
+// per-surface drop-in (batch.rs:23-42: one launch per parameter set) and the
+// batched multi-surface launch, so a contract's price is bit-identical
+// whichever way, and whatever else, it is launched with.
 //
 // Work unit = one Gil-Pelaez integral of one contract (P1 or P2,
 // heston.rs:92-93 / bates.rs:58-59), integrated by one warp.  The two
@@ -12,6 +15,16 @@
 
 #include "internal.h"
 #include "quadrature.cuh"
+
+// Launch shape of the pricing kernel: warps per block and the minimum resident
+// blocks per SM handed to __launch_bounds__ (which caps registers per thread
+// at 65536 / (32 * WARPS * MINB)).
+#ifndef OPE_KERNEL_WARPS
+#define OPE_KERNEL_WARPS 4
+#endif
+#ifndef OPE_KERNEL_MINB
+#define OPE_KERNEL_MINB 1
+#endif
 
 namespace ope {
 
@@ -77,21 +90,6 @@ __device__ __forceinline__ void run_unit(long long c, int which, const ope_contr
     }
 }
 
-// Plain launch: one warp per unit, one parameter set (a single batch_* call).
-template <bool BATES>
-__global__ void __launch_bounds__(128) k_price_plain(const ope_contract* __restrict__ con, long long n,
-                                                     const double* __restrict__ params, double tol,
-                                                     double* __restrict__ out, double* integ,
-                                                     unsigned int* done, int32_t* nbis_out) {
-    extern __shared__ PanelStore smem_panels[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const long long unit = (long long)blockIdx.x * (blockDim.x >> 5) + warp;
-    if (unit >= 2 * n) return;
-    const LaneRule R = lane_rule(lane);
-    run_unit<BATES>(unit >> 1, (int)(unit & 1), con, params, tol, out, integ, done, nbis_out, smem_panels[warp],
-                    lane, R);
-}
-
 // Surface of contract c: the s with off[s] <= c < off[s+1] (upper_bound - 1).
 __device__ __forceinline__ long long find_surface(const int64_t* off, long long n_surf, long long c) {
     long long lo = 1, hi = n_surf;  // search [1, n_surf] for the first off[j] > c
@@ -102,10 +100,10 @@ __device__ __forceinline__ long long find_surface(const int64_t* off, long long 
     return lo - 1;
 }
 
-// Persistent launch: a grid sized to the resident capacity; every warp pulls
-// units from the device queue until it drains.
+// Every warp pulls units from the device queue until it drains; the grid is
+// the resident capacity of the GPU, or fewer warps than units for small calls.
 template <bool BATES>
-__global__ void __launch_bounds__(128) k_price_persistent(const ope_contract* __restrict__ con, long long n,
+__global__ void __launch_bounds__(OPE_KERNEL_WARPS * 32, OPE_KERNEL_MINB) k_price_persistent(const ope_contract* __restrict__ con, long long n,
                                                           const int64_t* __restrict__ surf_off, long long n_surf,
                                                           const int32_t* __restrict__ param_idx,
                                                           const double* __restrict__ params, double tol,
@@ -142,33 +140,13 @@ int persistent_grid(K kernel, int threads, size_t smem, int* grid) {
 
 }  // namespace
 
-int launch_price_plain(int model, const ope_contract* con, size_t n, const double* params, double tol,
-                       double* out, const PriceScratch& s, cudaStream_t st, int32_t* nbis_out) {
-    if (n == 0) return OPE_OK;
-    OPE_CHECK(cudaMemsetAsync(s.done, 0, n * sizeof(unsigned int), st));
-    const int warps = 4, threads = warps * 32;
-    const size_t smem = warps * sizeof(PanelStore);
-    const unsigned long long units = 2ull * n;
-    const unsigned int grid = (unsigned int)((units + warps - 1) / warps);
-    if (model == OPE_MODEL_BATES) {
-        OPE_CHECK(cudaFuncSetAttribute(k_price_plain<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_price_plain<true><<<grid, threads, smem, st>>>(con, (long long)n, params, tol, out, s.integ, s.done, nbis_out);
-    } else {
-        OPE_CHECK(cudaFuncSetAttribute(k_price_plain<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_price_plain<false><<<grid, threads, smem, st>>>(con, (long long)n, params, tol, out, s.integ, s.done, nbis_out);
-    }
-    OPE_CHECK(cudaGetLastError());
-    tctx().launches += 1;
-    return OPE_OK;
-}
-
 int launch_price_persistent(int model, const ope_contract* con, size_t n, const int64_t* surf_offsets,
                             size_t n_surf, const int32_t* param_idx, const double* params, double tol, double* out,
                             const PriceScratch& s, cudaStream_t st, int32_t* nbis_out) {
     if (n == 0) return OPE_OK;
     OPE_CHECK(cudaMemsetAsync(s.done, 0, n * sizeof(unsigned int), st));
     OPE_CHECK(cudaMemsetAsync(s.head, 0, sizeof(unsigned long long), st));
-    const int warps = 4, threads = warps * 32;
+    const int warps = OPE_KERNEL_WARPS, threads = warps * 32;
     const size_t smem = warps * sizeof(PanelStore);
     int grid = 0;
     if (model == OPE_MODEL_BATES) {

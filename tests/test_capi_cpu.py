@@ -1,0 +1,60 @@
+"""CPU: the C-ABI library loads, exports every symbol include/ope.h declares,
+and refuses to compute without a device (no CPU fallback)."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import HAS_GPU, ROOT
+
+
+def test_header_symbols_are_exported(ope):
+    from ope_b200 import _lib
+
+    declared = _lib.declared_symbols(os.path.join(ROOT, "include", "ope.h"))
+    assert len(declared) >= 15
+    L = _lib.load()
+    missing = [s for s in declared if not hasattr(L, s)]
+    assert not missing, missing
+
+
+def test_python_signatures_cover_header(ope):
+    from ope_b200 import _lib
+
+    declared = set(_lib.declared_symbols(os.path.join(ROOT, "include", "ope.h")))
+    assert declared <= set(_lib._SIGS), declared - set(_lib._SIGS)
+
+
+def test_record_layouts_match_header():
+    from ope_b200.api import RESULT_DTYPE
+    from ope_b200.workloads import CONTRACT_DTYPE
+
+    assert CONTRACT_DTYPE.itemsize == 56 and RESULT_DTYPE.itemsize == 64
+    assert list(CONTRACT_DTYPE.names) == ["spot", "strike", "expiry", "rate", "div_yield", "vol", "opt_type", "pad"]
+
+
+def test_library_is_sm100a_only():
+    import subprocess
+
+    so = os.path.join(ROOT, "options-pricing-engine-rs_b200", "lib", "libope_b200.so")
+    out = subprocess.run(["cuobjdump", "--list-elf", so], capture_output=True, text=True).stdout
+    assert "sm_100a" in out
+
+
+@pytest.mark.skipif(HAS_GPU, reason="checks the no-device error path")
+def test_no_device_fails_loudly(ope):
+    with pytest.raises(ope.OpeError) as e:
+        ope.heston_price(100.0, 100.0, 1.0, 0.03, 0.0, [0.04, 2.0, 0.04, 0.3, -0.7])
+    assert e.value.status == 4  # OPE_ERR_NO_DEVICE
+
+
+def test_empty_batch_needs_no_device(ope):
+    assert ope.batch_heston(np.zeros(0, ope.api.CONTRACT_DTYPE), [0.04, 2.0, 0.04, 0.3, -0.7]).size == 0
+
+
+def test_api_rejects_wrong_param_shapes(ope):
+    with pytest.raises(ValueError):
+        ope.batch_bates(np.zeros(1, ope.api.CONTRACT_DTYPE), [0.04, 2.0, 0.04, 0.3, -0.7])
+    with pytest.raises(ValueError):
+        ope.price_surfaces(ope.MODEL_HESTON, np.zeros(2, ope.api.CONTRACT_DTYPE), [0, 1, 2],
+                           [[0.04, 2.0, 0.04, 0.3, -0.7]])
