@@ -139,6 +139,15 @@ int ope_price_surfaces(int32_t model, const ope_contract* contracts, size_t n,
                        const int64_t* surf_offsets, size_t n_surf, const void* params,
                        double* out_prices, const ope_options* opts);
 
+/* ad.rs:695-731 forward_pass (all parameters at once) / ad.rs:882-895
+ * bates_jump_sensitivities_ad, batched over surfaces like ope_price_surfaces:
+ * prices plus d price / d params by a reverse-mode adjoint kernel over the
+ * primal's final panel set.  out_grad is n x dim, dim = 5 for Heston
+ * (v0, kappa, theta, sigma, rho) and 8 for Bates (+ lambda, mu_j, sigma_j). */
+int ope_price_gradient_surfaces(int32_t model, const ope_contract* contracts, size_t n,
+                                const int64_t* surf_offsets, size_t n_surf, const void* params,
+                                double* out_prices, double* out_grad, const ope_options* opts);
+
 /* ope_price_surfaces plus diagnostics: out_bisections (may be NULL) receives
  * 2n int32 — the bisection count of each contract's P1 and P2 integral (the
  * loop iterations of heston.rs:200-210), from which the nodes evaluated are
@@ -151,6 +160,11 @@ int ope_price_surfaces_stats(int32_t model, const ope_contract* contracts, size_
  * measured by a DFMA-chain kernel (2 flops per DFMA) on the calling thread's
  * device.  The roofline denominator for the FP64-bound pricing kernels. */
 int ope_measure_fp64_peak(double* flops_per_s, double* elapsed_ms);
+
+/* No reference twin (numerics self-check): the worst error, in ulps, of the
+ * kernels' Newton-refined reciprocal and square root against IEEE 1/x and
+ * sqrt over 2^20 inputs spanning 1e-300 .. 1e300. */
+int ope_selftest_math(uint64_t* max_ulp_rcp, uint64_t* max_ulp_sqrt);
 
 #ifdef __cplusplus
 } /* extern "C" */

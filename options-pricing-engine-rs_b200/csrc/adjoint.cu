@@ -1,0 +1,177 @@
+// Price + reverse-mode gradient kernel: d price / d(v0, kappa, theta, sigma,
+// rho[, lambda, mu_j, sigma_j]) for every contract of many surfaces.
+//
+// Reference: ad.rs:695-731 (forward_pass: derivative integrated by Leibniz
+// over the primal's adaptive panel set, error control on the primal only),
+// ad.rs:736-745 / 821-825 (the five Heston-parameter passes) and ad.rs:882-895
+// (the three jump-parameter passes).  One unit = one integral, one warp:
+//   1. the primal greedy GK15 integration (identical to the pricing kernel),
+//      leaving the final live-panel list in shared memory;
+//   2. the derivative integral over those panels: the 15 * len nodes are
+//      spread over the 32 lanes, each lane recomputes the CF at its node and
+//      runs the backward pass (cf_adjoint.cuh), accumulating all parameter
+//      derivatives at once; a warp reduction finishes the sums.
+// The price combination is heston.rs:95-98 and the derivative combination is
+// ad.rs:713-730: d price = S e^{-qT} dI1/pi - K e^{-rT} dI2/pi for calls and
+// puts alike (parity terms do not depend on the model parameters).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "cf_adjoint.cuh"
+#include "internal.h"
+#include "quadrature.cuh"
+
+namespace ope {
+
+namespace {
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    return v;
+}
+
+__device__ __forceinline__ long long find_surface_g(const int64_t* off, long long n_surf, long long c) {
+    long long lo = 1, hi = n_surf;
+    while (lo < hi) {
+        const long long mid = (lo + hi) >> 1;
+        if (__ldg(off + mid) > c) hi = mid; else lo = mid + 1;
+    }
+    return lo - 1;
+}
+
+template <bool BATES>
+__global__ void __launch_bounds__(128) k_price_grad(const ope_contract* __restrict__ con, long long n,
+                                                    const int64_t* __restrict__ surf_off, long long n_surf,
+                                                    const int32_t* __restrict__ param_idx,
+                                                    const double* __restrict__ params, double tol,
+                                                    double* __restrict__ out_price, double* __restrict__ out_grad,
+                                                    double* integ, double* ginteg, unsigned int* done,
+                                                    unsigned long long* head) {
+    constexpr int DIM = BATES ? 8 : 5;
+    extern __shared__ PanelStore smem_panels[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    PanelStore& L = smem_panels[warp];
+    const LaneRule R = lane_rule(lane);
+    const unsigned long long n_units = 2ull * (unsigned long long)n;
+    while (true) {
+        unsigned long long unit = 0;
+        if (lane == 0) unit = atomicAdd(head, 1ull);
+        unit = __shfl_sync(0xffffffffu, unit, 0);
+        if (unit >= n_units) break;
+        const long long c = (long long)(unit >> 1);
+        const int which = (int)(unit & 1);
+        const long long s = param_idx ? (long long)__ldg(param_idx + c)
+                                      : (n_surf > 1 ? find_surface_g(surf_off, n_surf, c) : 0);
+        const double* p = params + s * DIM;
+        double pl[8];
+#pragma unroll
+        for (int i = 0; i < DIM; ++i) pl[i] = __ldg(p + i);
+        const ope_contract* cp = con + c;
+        const double S = __ldg(&cp->spot), K = __ldg(&cp->strike), T = __ldg(&cp->expiry), r = __ldg(&cp->rate),
+                     q = __ldg(&cp->div_yield);
+        const int ot = __ldg(&cp->opt_type);
+        const CfConsts C = make_consts(S, K, T, r, pl, BATES, which);
+        int nb;
+        const double I = gk_integrate_warp<BATES>(C, tol, L, lane, R, &nb);
+        const int len = nb + 1;
+
+        // derivative integral over the final panel set
+        const GradParams G = make_grad_params(pl, BATES);
+        double acc[DIM];
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) acc[k] = 0.0;
+        double sw_re = 0.0, sw_im = 0.0;
+        const int total = 15 * len;
+        for (int base = 0; base < total; base += 32) {
+            const int idx = base + lane;
+            const int pi = idx / 15, j = idx - 15 * (idx / 15);
+            const double xj = __shfl_sync(0xffffffffu, R.x, j & 15);
+            const double wj = __shfl_sync(0xffffffffu, R.wk, j & 15);
+            if (idx < total) {
+                const double a = L.a[pi], b = L.b[pi];
+                const double cc = 0.5 * (a + b), h = 0.5 * (b - a);
+                const double tn = __dadd_rn(cc, __dmul_rn(h, xj));
+                node_grad<BATES>(C, G, tn, h * wj, acc, sw_re, sw_im);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) acc[k] = warp_sum(acc[k]);
+        sw_re = warp_sum(sw_re);
+        sw_im = warp_sum(sw_im);
+        if (which == 0) {
+            // -d Log CF(-i)/dp, constant over the integral (zero up to rounding for a
+            // regular normaliser; ad.rs:705-706 carries it through the Dual division)
+            C2 dlm[8];
+            exponent_and_grad<BATES>(C, G, 0.0, dlm);
+#pragma unroll
+            for (int k = 0; k < DIM; ++k) acc[k] -= (dlm[k] * c2(sw_re, sw_im)).im;
+        }
+        if (lane == 0) {
+            integ[2 * c + which] = I;
+#pragma unroll
+            for (int k = 0; k < DIM; ++k) ginteg[(2 * c + which) * DIM + k] = acc[k];
+            __threadfence();
+            const unsigned int prev = atomicAdd(done + c, 1u);
+            if (prev == 1u) {
+                __threadfence();
+                const int o = 1 - which;
+                const double other = __ldcg(integ + 2 * c + o);
+                const double i1 = which == 0 ? I : other, i2 = which == 0 ? other : I;
+                out_price[c] = finish_price(S, K, T, r, q, ot, i1, i2);
+                const double PI = 3.14159265358979323846;
+                const double seq = S * exp(-q * T), ker = K * exp(-r * T);
+#pragma unroll
+                for (int k = 0; k < DIM; ++k) {
+                    const double og = __ldcg(ginteg + (2 * c + o) * DIM + k);
+                    const double d1 = which == 0 ? acc[k] : og, d2 = which == 0 ? og : acc[k];
+                    out_grad[c * DIM + k] = seq * (d1 / PI) - ker * (d2 / PI);
+                }
+            }
+        }
+    }
+}
+
+template <class K>
+int grad_grid(K kernel, size_t smem, unsigned long long need, int* grid) {
+    int per_sm = 0;
+    OPE_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    OPE_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 128, smem));
+    if (per_sm < 1) per_sm = 1;
+    *grid = (int)std::min<unsigned long long>((unsigned long long)per_sm * tctx().sm_count, need);
+    return OPE_OK;
+}
+
+}  // namespace
+
+size_t grad_scratch_bytes(size_t n, int dim) {
+    return price_scratch_bytes(n) + align_up(2 * n * dim * sizeof(double), 256);
+}
+
+int launch_price_grad(int model, const ope_contract* con, size_t n, const int64_t* surf_offsets, size_t n_surf,
+                      const int32_t* param_idx, const double* params, double tol, double* out_price,
+                      double* out_grad, void* scratch, cudaStream_t st) {
+    if (n == 0) return OPE_OK;
+    const PriceScratch s = carve_price_scratch(scratch, n);
+    double* ginteg = reinterpret_cast<double*>(static_cast<char*>(scratch) + price_scratch_bytes(n));
+    OPE_CHECK(cudaMemsetAsync(s.done, 0, n * sizeof(unsigned int), st));
+    OPE_CHECK(cudaMemsetAsync(s.head, 0, sizeof(unsigned long long), st));
+    const size_t smem = 4 * sizeof(PanelStore);
+    const unsigned long long need = (2ull * n + 3) / 4;
+    int grid = 0;
+    if (model == OPE_MODEL_BATES) {
+        OPE_TRY(grad_grid(k_price_grad<true>, smem, need, &grid));
+        k_price_grad<true><<<grid, 128, smem, st>>>(con, (long long)n, surf_offsets, (long long)n_surf, param_idx,
+                                                    params, tol, out_price, out_grad, s.integ, ginteg, s.done, s.head);
+    } else {
+        OPE_TRY(grad_grid(k_price_grad<false>, smem, need, &grid));
+        k_price_grad<false><<<grid, 128, smem, st>>>(con, (long long)n, surf_offsets, (long long)n_surf, param_idx,
+                                                     params, tol, out_price, out_grad, s.integ, ginteg, s.done, s.head);
+    }
+    OPE_CHECK(cudaGetLastError());
+    tctx().launches += 1;
+    return OPE_OK;
+}
+
+}  // namespace ope

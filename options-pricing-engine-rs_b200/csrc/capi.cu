@@ -243,6 +243,57 @@ int ope_batch_greeks_ex(int32_t model, const ope_contract* contracts, size_t n, 
     return batch_greeks(model, contracts, n, params, out, opts);
 }
 
+int ope_price_gradient_surfaces(int32_t model, const ope_contract* contracts, size_t n, const int64_t* surf_offsets,
+                                size_t n_surf, const void* params, double* out_prices, double* out_grad,
+                                const ope_options* opts) {
+    OPE_TRY(check_model(model));
+    double tol;
+    OPE_TRY(resolve_tol(opts, &tol));
+    if (n == 0) return OPE_OK;
+    if (!contracts || !params || !out_prices || !out_grad || !surf_offsets)
+        return set_error(OPE_ERR_INVALID_ARG, "NULL array argument");
+    if (n_surf == 0) return set_error(OPE_ERR_INVALID_ARG, "n_surf must be >= 1 when n > 0");
+    OPE_TRY(ensure_device());
+    const int dim = param_stride(model);
+    if (device_ptrs(opts)) {
+        void* ws;
+        OPE_TRY(ensure_workspace(grad_scratch_bytes(n, dim), &ws));
+        return launch_price_grad(model, contracts, n, surf_offsets, n_surf, nullptr, static_cast<const double*>(params),
+                                 tol, out_prices, out_grad, ws, user_stream(opts));
+    }
+    if (surf_offsets[0] != 0 || surf_offsets[n_surf] != (int64_t)n)
+        return set_error(OPE_ERR_INVALID_ARG, "surf_offsets must start at 0 and end at n");
+    for (size_t s = 0; s < n_surf; ++s)
+        if (surf_offsets[s + 1] < surf_offsets[s]) return set_error(OPE_ERR_INVALID_ARG, "surf_offsets not sorted");
+    ThreadCtx& c = tctx();
+    const size_t b_con = align_up(n * sizeof(ope_contract), 256), b_off = align_up((n_surf + 1) * sizeof(int64_t), 256),
+                 b_par = align_up(n_surf * dim * sizeof(double), 256), b_out = align_up(n * sizeof(double), 256),
+                 b_g = align_up(n * dim * sizeof(double), 256);
+    void* ws;
+    OPE_TRY(ensure_workspace(b_con + b_off + b_par + b_out + b_g + grad_scratch_bytes(n, dim), &ws));
+    char* p = static_cast<char*>(ws);
+    ope_contract* d_con = reinterpret_cast<ope_contract*>(p);
+    int64_t* d_off = reinterpret_cast<int64_t*>(p + b_con);
+    double* d_par = reinterpret_cast<double*>(p + b_con + b_off);
+    double* d_out = reinterpret_cast<double*>(p + b_con + b_off + b_par);
+    double* d_g = reinterpret_cast<double*>(p + b_con + b_off + b_par + b_out);
+    void* scratch = p + b_con + b_off + b_par + b_out + b_g;
+    OPE_CHECK(cudaMemcpyAsync(d_con, contracts, n * sizeof(ope_contract), cudaMemcpyHostToDevice, c.stream));
+    OPE_CHECK(cudaMemcpyAsync(d_off, surf_offsets, (n_surf + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, c.stream));
+    OPE_CHECK(cudaMemcpyAsync(d_par, params, n_surf * dim * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    OPE_TRY(launch_price_grad(model, d_con, n, d_off, n_surf, nullptr, d_par, tol, d_out, d_g, scratch, c.stream));
+    OPE_CHECK(cudaMemcpyAsync(out_prices, d_out, n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    OPE_CHECK(cudaMemcpyAsync(out_grad, d_g, n * dim * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    OPE_CHECK(cudaStreamSynchronize(c.stream));
+    return OPE_OK;
+}
+
+int ope_selftest_math(uint64_t* max_ulp_rcp, uint64_t* max_ulp_sqrt) {
+    if (!max_ulp_rcp || !max_ulp_sqrt) return set_error(OPE_ERR_INVALID_ARG, "NULL argument");
+    OPE_TRY(ensure_device());
+    return selftest_math(max_ulp_rcp, max_ulp_sqrt);
+}
+
 int ope_measure_fp64_peak(double* flops_per_s, double* elapsed_ms) {
     if (!flops_per_s || !elapsed_ms) return set_error(OPE_ERR_INVALID_ARG, "NULL argument");
     OPE_TRY(ensure_device());

@@ -1,0 +1,171 @@
+// Reverse-mode derivative of one Gil-Pelaez node with respect to the model
+// parameters (v0, kappa, theta, sigma, rho[, lambda, mu_j, sigma_j]).
+//
+// Reference: ad.rs:609-731 (forward-mode Dual through stable_cf_dual,
+// jump_factor and dual_integrand, integrated over the primal's adaptive
+// panel set).  Same quantity, computed backwards: the node value is
+//
+//     g(t) = Im(W) / (u t^2),  W = exp(Z),  Z = kts*Ch + v0s*Dh + i r phi T + i u x - Log CF(-i) [+ J]
+//
+// with Ch = (xi-d)T - 2 Log A and Dh = (xi-d)(1-e)/(1-g e) (the C and D of
+// heston.rs:123-124 without their real prefactors kappa*theta/sigma^2 and
+// v0/sigma^2).  Every intermediate is a holomorphic function of the two
+// complex inputs xi and z = xi^2 + sigma^2 phi(phi+i), so the whole backward
+// pass reduces to two complex partials Z_xi, Z_z (chain rule through
+// d = sqrt z, g = (xi-d)/(xi+d), e = exp(-dT), A = (ge-1)/(g-1)), which are
+// then chained to each real parameter:
+//
+//   dZ/dv0    = Dh / sigma^2
+//   dZ/dkappa = Y + Ch * theta / sigma^2          Y = Z_xi + 2 xi Z_z
+//   dZ/dtheta = Ch * kappa / sigma^2
+//   dZ/dsigma = Y rho s + Z_z 2 sigma w - 2 kts Ch / sigma - 2 v0s Dh / sigma
+//   dZ/drho   = Y sigma s                          s = phi_im - i u, w = phi(phi+i)
+//
+// and dg/dp = Im(W dZ/dp) / (u t^2).  The CF is recomputed here, nothing from
+// the primal pass is stored.  The P1 normaliser term -dLog CF(-i)/dp is the
+// same expression at phi = -i; since it is constant over the integral its
+// contribution is applied once per integral to the sum of W/(u t^2) weights.
+#pragma once
+
+#include "cf_device.cuh"
+
+namespace ope {
+
+struct C2 {
+    double re, im;
+};
+__device__ __forceinline__ C2 c2(double re, double im) { return C2{re, im}; }
+__device__ __forceinline__ C2 operator+(C2 a, C2 b) { return C2{a.re + b.re, a.im + b.im}; }
+__device__ __forceinline__ C2 operator-(C2 a, C2 b) { return C2{a.re - b.re, a.im - b.im}; }
+__device__ __forceinline__ C2 operator*(C2 a, C2 b) { return C2{a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+__device__ __forceinline__ C2 operator*(C2 a, double s) { return C2{a.re * s, a.im * s}; }
+__device__ __forceinline__ C2 operator*(double s, C2 a) { return C2{a.re * s, a.im * s}; }
+__device__ __forceinline__ C2 crcp(C2 a) {
+    const double inv = 1.0 / (a.re * a.re + a.im * a.im);
+    return C2{a.re * inv, -a.im * inv};
+}
+
+// Real model parameters for the chain to (v0, kappa, theta, sigma, rho, ...).
+struct GradParams {
+    double v0, kappa, theta, sigma, rho;
+    double sigma_j;
+};
+
+__device__ __forceinline__ GradParams make_grad_params(const double* p, bool bates) {
+    GradParams G;
+    G.v0 = p[0];
+    G.kappa = p[1];
+    G.theta = p[2];
+    G.sigma = p[3];
+    G.rho = p[4];
+    G.sigma_j = bates ? p[7] : 0.0;
+    return G;
+}
+
+// dZ/dp at (u, phi_im) for every parameter (dim = 5 or 8), plus W = exp(Z)
+// (W only meaningful for u > 0).  `out` receives dZ/dp as complex numbers.
+template <bool BATES>
+__device__ __forceinline__ C2 exponent_and_grad(const CfConsts& C, const GradParams& P, double u, C2* out) {
+    const double T = C.t;
+    const C2 xi = c2(C.kappa + C.rs * C.phi_im, -C.rs * u);
+    const C2 wphi = c2(u * u, C.sgn * u);  // phi(phi+i)
+    const C2 z = xi * xi + wphi * C.sig2;
+    const Cx dd = fast_csqrt(z.re, z.im);
+    const C2 d = c2(dd.re, dd.im);
+    const C2 m = xi - d, p = xi + d;
+    const C2 ip = crcp(p);
+    const C2 g = m * ip;
+    double sn, cs;
+    sincos(-d.im * T, &sn, &cs);
+    const double em = exp(-d.re * T);
+    const C2 e = c2(em * cs, em * sn);
+    const C2 ge = g * e;
+    const C2 N = c2(ge.re - 1.0, ge.im);  // g e - 1  (= -(1 - g e))
+    const C2 M = c2(g.re - 1.0, g.im);    // g - 1
+    const C2 iM = crcp(M);
+    const C2 iN = crcp(N);
+    const C2 A = N * iM;
+    const C2 lnA = c2(0.5 * log(A.re * A.re + A.im * A.im), atan2(A.im, A.re));
+    const C2 om = c2(1.0 - e.re, -e.im);  // 1 - e
+    const C2 iQ = c2(-iN.re, -iN.im);     // 1/(1 - g e)
+    const C2 Ch = m * T - lnA * 2.0;
+    const C2 Dh = m * om * iQ;
+    // Z (without the Log CF(-i) normaliser, added by the caller through C.lnm)
+    C2 Z = Ch * C.kts + Dh * C.v0s + c2(-C.rt * C.phi_im + C.lnm_re, C.rt * u + u * C.x + C.lnm_im);
+
+    // backward: holomorphic partials through d, g, e, A
+    const C2 ip2 = ip * ip;
+    const C2 g_xi = d * ip2 * 2.0;
+    const C2 g_d = xi * ip2 * (-2.0);
+    const C2 e_d = e * (-T);
+    const C2 iMN = iM * iN;
+    const C2 C_xi = (c2(T, 0.0) - om * g_xi * iMN * 2.0) * C.kts;
+    const C2 C_d = (c2(-T, 0.0) - (om * g_d * iMN + g * e_d * iN) * 2.0) * C.kts;
+    const C2 iQ2 = iQ * iQ;
+    const C2 mom = m * om;
+    const C2 D_xi = (om * iQ + mom * e * g_xi * iQ2) * C.v0s;
+    const C2 D_d = (c2(-om.re, -om.im) * iQ - m * e_d * iQ + mom * (g_d * e + g * e_d) * iQ2) * C.v0s;
+    const C2 Z_xi = C_xi + D_xi;
+    const C2 Z_z = (C_d + D_d) * crcp(d * 2.0);
+    const C2 Y = Z_xi + xi * Z_z * 2.0;
+    const C2 s = c2(C.phi_im, -u);
+    const double is2 = 1.0 / C.sig2;
+    out[0] = Dh * is2;                                                     // v0
+    out[1] = Y + Ch * (P.theta * is2);                                     // kappa
+    out[2] = Ch * (P.kappa * is2);                                         // theta
+    out[3] = Y * s * P.rho + Z_z * wphi * (2.0 * P.sigma) - Ch * (2.0 * C.kts / P.sigma) -
+             Dh * (2.0 * C.v0s / P.sigma);                                 // sigma
+    out[4] = Y * s * P.sigma;                                              // rho
+    if (BATES) {
+        const C2 iphi = c2(-C.phi_im, u);
+        const C2 phi2 = c2(u * u - C.phi_im * C.phi_im, 2.0 * u * C.phi_im);
+        const double jr_in = -C.phi_im * C.mu_j - C.hs2 * phi2.re;
+        const double ji_in = u * C.mu_j - C.hs2 * phi2.im;
+        double js, jc;
+        sincos(ji_in, &js, &jc);
+        const double je = exp(jr_in);
+        const C2 jump = c2(je * jc, je * js);
+        const C2 base = jump - c2(1.0, 0.0) - iphi * C.comp;
+        Z = Z + base * C.lt;
+        out[5] = base * T;                                                            // lambda
+        out[6] = iphi * (jump - c2(1.0 + C.comp, 0.0)) * C.lt;                        // mu_j
+        out[7] = (c2(-(jump * phi2).re, -(jump * phi2).im) - iphi * (1.0 + C.comp)) *
+                 (C.lt * P.sigma_j);                                                  // sigma_j
+    }
+    return Z;
+}
+
+// One node of the derivative integral: returns g(t) and adds hw * dg/dp into
+// acc[0..dim); adds hw * W/(u t^2) into sw (for the P1 normaliser term).
+// A node whose value or derivative is not finite contributes zero, as in
+// gk_integrate_dual (ad.rs:679-682).
+template <bool BATES>
+__device__ __forceinline__ double node_grad(const CfConsts& C, const GradParams& P, double tn, double hw, double* acc,
+                                            double& sw_re, double& sw_im) {
+    constexpr int DIM = BATES ? 8 : 5;
+    const double u = (1.0 - tn) / tn;
+    C2 dz[8];
+    const C2 Z = exponent_and_grad<BATES>(C, P, u, dz);
+    double sn, cs;
+    sincos(Z.im, &sn, &cs);
+    const double ez = exp(Z.re);
+    const double scale = 1.0 / (u * (tn * tn));
+    const C2 Wf = c2(ez * cs * scale, ez * sn * scale);
+    const double v = Wf.im;
+    bool ok = (tn > 0.0) && (u >= 1e-12) && isfinite(v);
+    double gk[8];
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) {
+        gk[k] = (Wf * dz[k]).im;
+        ok = ok && isfinite(gk[k]);
+    }
+    if (ok) {
+#pragma unroll
+        for (int k = 0; k < DIM; ++k) acc[k] += hw * gk[k];
+        sw_re += hw * Wf.re;
+        sw_im += hw * Wf.im;
+    }
+    return ok ? v : 0.0;
+}
+
+}  // namespace ope

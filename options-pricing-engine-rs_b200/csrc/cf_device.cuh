@@ -33,6 +33,33 @@ struct Cx {
     double re, im;
 };
 
+// Reciprocal and reciprocal square root: the hardware approximation
+// (rcp/rsqrt.approx.ftz.f64, about 2^-22 relative error) refined by two
+// Newton-Raphson steps, y <- y + y(1 - x y) and y <- y + y(1/2 - x y^2 / 2),
+// each of which squares the relative error, so the result is within an ulp
+// or two of the correctly rounded value (checked against IEEE division and
+// sqrt by ope_selftest_math).  Used for the complex reciprocals and the
+// square root of the node evaluation; a zero or infinite argument gives a
+// non-finite result, which zeroes the node exactly as the reference's
+// division by zero does.
+__device__ __forceinline__ double rcp_nr(double x) {
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    double e = fma(-x, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-x, y, 1.0);
+    return fma(y, e, y);
+}
+__device__ __forceinline__ double rsqrt_nr(double x) {
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    const double hx = 0.5 * x;
+    double e = fma(-hx * y, y, 0.5);
+    y = fma(y, e, y);
+    e = fma(-hx * y, y, 0.5);
+    return fma(y, e, y);
+}
+
 __device__ __forceinline__ Cx cadd(Cx a, Cx b) { return Cx{a.re + b.re, a.im + b.im}; }
 __device__ __forceinline__ Cx csub(Cx a, Cx b) { return Cx{a.re - b.re, a.im - b.im}; }
 __device__ __forceinline__ Cx cmul(Cx a, Cx b) {
@@ -62,25 +89,18 @@ __device__ __forceinline__ Cx fast_csqrt(double a, double b) {
     return (a >= 0.0) ? Cx{w, q} : Cx{fabs(q), copysign(w, b)};
 }
 
-// Per-integral constants (everything that does not depend on the node).
+// Per-integral constants (everything that does not depend on the node),
+// folded so that the node evaluation does as little as possible:
+//   xi   = (xr, -rs u)                       xi = kappa - i rho sigma phi, phi = u + i phi_im
+//   z    = xi^2 + (sig2 u^2, sig2s u)       sigma^2 phi(phi+i)
+//   Re Z = kts Re Ch + v0s Re Dh + z0re      z0re = r T + Re(-Log CF(-i)) for P1, 0 for P2
+//   Im Z = kts Im Ch + v0s Im Dh + rtx u + z0im      rtx = r T + ln(S/K)
+//   Bates: jump = exp(jr0 - hs2 u^2 + i jmu u);  J = (lt Re jump + jre0, lt Im jump - ltc u)
 struct CfConsts {
-    double kappa;    // kappa
-    double rs;       // rho * sigma
-    double sig2;     // sigma^2
-    double kts;      // kappa * theta / sigma^2
-    double v0s;      // v0 / sigma^2
-    double t;        // expiry T
-    double rt;       // r * T
-    double x;        // ln(S/K)
-    double phi_im;   // -1 for P1 (phi = u - i), 0 for P2 (phi = u)
-    double sgn;      // Im of phi*(phi+i) / u: -1 for P1, +1 for P2
-    double lnm_re;   // -Re Log CF(-i) for P1, 0 for P2
-    double lnm_im;   // -Im Log CF(-i) for P1, 0 for P2
-    // Bates (bates.rs:77-83); lt = 0 switches the jump factor off.
-    double lt;       // lambda * T
-    double mu_j;     // mu_j
-    double hs2;      // 0.5 * sigma_j^2
-    double comp;     // e^{mu_j + sigma_j^2/2} - 1
+    double xr, rs, sig2, sig2s, kts, v0s, t, rtx, z0re, z0im;
+    double jr0, hs2, jmu, lt, jre0, ltc;
+    // raw values kept for the adjoint chain
+    double kappa, phi_im, sgn, rt, x, lnm_re, lnm_im, mu_j, comp;
 };
 
 // stable_cf at a general complex phi, following heston.rs:113-127's operation
@@ -131,17 +151,24 @@ __device__ __forceinline__ CfConsts make_consts(double s, double k, double t, do
     C.x = log(s / k);
     C.phi_im = (which == 0) ? -1.0 : 0.0;
     C.sgn = (which == 0) ? -1.0 : 1.0;
+    C.xr = kappa + C.rs * C.phi_im;
+    C.sig2s = C.sig2 * C.sgn;
+    C.rtx = C.rt + C.x;
+    double lt = 0.0, mu_j = 0.0, hs2 = 0.0, comp = 0.0;
     if (bates) {
-        C.lt = p[5] * t;
-        C.mu_j = p[6];
-        C.hs2 = 0.5 * p[7] * p[7];
-        C.comp = exp(p[6] + (0.5 * p[7]) * p[7]) - 1.0;
-    } else {
-        C.lt = 0.0;
-        C.mu_j = 0.0;
-        C.hs2 = 0.0;
-        C.comp = 0.0;
+        lt = p[5] * t;
+        mu_j = p[6];
+        hs2 = 0.5 * p[7] * p[7];
+        comp = exp(p[6] + (0.5 * p[7]) * p[7]) - 1.0;
     }
+    C.lt = lt;
+    C.mu_j = mu_j;
+    C.hs2 = hs2;
+    C.comp = comp;
+    C.jr0 = -C.phi_im * mu_j + hs2 * (C.phi_im * C.phi_im);
+    C.jmu = mu_j - 2.0 * hs2 * C.phi_im;
+    C.jre0 = lt * (C.phi_im * comp - 1.0);
+    C.ltc = lt * comp;
     C.lnm_re = 0.0;
     C.lnm_im = 0.0;
     if (which == 0) {
@@ -152,68 +179,75 @@ __device__ __forceinline__ CfConsts make_consts(double s, double k, double t, do
         C.lnm_re = -lm.re;
         C.lnm_im = -lm.im;
     }
+    C.z0re = -C.rt * C.phi_im + C.lnm_re;
+    C.z0im = C.lnm_im;
     return C;
 }
 
 // gk_integrate's g(t) (heston.rs:221-227) with the merged-exponent integrand.
 template <bool BATES>
 __device__ __forceinline__ double node_value(const CfConsts& C, double tn) {
-    const double u = (1.0 - tn) / tn;
-    // xi = kappa - i*rho*sigma*phi,  phi = u + i*phi_im
-    const double xr = C.kappa + C.rs * C.phi_im;
-    const double xi = -C.rs * u;
-    // z = xi^2 + sigma^2 * phi*(phi+i);  phi*(phi+i) = (u^2, sgn*u) for both integrals
-    const double zr = (xr * xr - xi * xi) + C.sig2 * (u * u);
-    const double zi = 2.0 * xr * xi + C.sig2 * (C.sgn * u);
-    const Cx d = fast_csqrt(zr, zi);
-    const double amr = xr - d.re, ami = xi - d.im;  // xi - d
-    const double apr = xr + d.re, api = xi + d.im;  // xi + d
+    const double it = rcp_nr(tn);
+    const double omt = 1.0 - tn;
+    const double u = omt * it;  // (1 - t) / t
+    const double u2 = u * u;
+    // xi = (xr, xi_) ; z = xi^2 + sigma^2 phi(phi+i)
+    const double xr = C.xr, xi_ = -C.rs * u;
+    const double zr = fma(xr, xr, fma(-xi_, xi_, C.sig2 * u2));
+    const double zi = fma(2.0 * xr, xi_, C.sig2s * u);
+    // d = fast_csqrt(z) (heston.rs:155-175): w = sqrt((|zr| + |z|)/2), other = zi / (2 w)
+    const double r = sqrt(fma(zr, zr, zi * zi));
+    const double s2 = 0.5 * (r + fabs(zr));
+    const double iw = rsqrt_nr(s2);
+    const double w = (s2 > 0.0) ? s2 * iw : 0.0;
+    const double q = (s2 > 0.0) ? (0.5 * zi) * iw : zi;
+    const double dre = (zr >= 0.0) ? w : fabs(q);
+    const double dim = (zr >= 0.0) ? q : copysign(w, zi);
+    const double amr = xr - dre, ami = xi_ - dim;  // xi - d
+    const double apr = xr + dre, api = xi_ + dim;  // xi + d
     // g = (xi - d) / (xi + d)
-    const double ig = 1.0 / (apr * apr + api * api);
-    const double gr = (amr * apr + ami * api) * ig;
-    const double gi = (ami * apr - amr * api) * ig;
+    const double ig = rcp_nr(fma(apr, apr, api * api));
+    const double gr = fma(amr, apr, ami * api) * ig;
+    const double gi = fma(ami, apr, -amr * api) * ig;
     // e = exp(-d T)
     double sn, cs;
-    sincos(-d.im * C.t, &sn, &cs);
-    const double em = exp(-d.re * C.t);
+    sincos(-dim * C.t, &sn, &cs);
+    const double em = exp(-dre * C.t);
     const double er = em * cs, ei = em * sn;
     // g e
-    const double ger = gr * er - gi * ei;
-    const double gei = gr * ei + gi * er;
+    const double ger = fma(gr, er, -gi * ei);
+    const double gei = fma(gr, ei, gi * er);
     // A = (g e - 1) / (g - 1)
     const double nr = ger - 1.0, ni = gei;
     const double dr = gr - 1.0, di = gi;
-    const double ia = 1.0 / (dr * dr + di * di);
-    const double ar = (nr * dr + ni * di) * ia;
-    const double ai = (ni * dr - nr * di) * ia;
+    const double ia = rcp_nr(fma(dr, dr, di * di));
+    const double ar = fma(nr, dr, ni * di) * ia;
+    const double ai = fma(ni, dr, -nr * di) * ia;
     // Log A
-    const double lr = 0.5 * log(ar * ar + ai * ai);
+    const double lr = 0.5 * log(fma(ar, ar, ai * ai));
     const double li = atan2(ai, ar);
-    // D = v0/sigma^2 * (xi - d)(1 - e) / (1 - g e)
+    // Dh = (xi - d)(1 - e) / (1 - g e)
     const double omr = 1.0 - er, omi = -ei;
-    const double pr = amr * omr - ami * omi;
-    const double pim = amr * omi + ami * omr;
+    const double pr = fma(amr, omr, -ami * omi);
+    const double pim = fma(amr, omi, ami * omr);
     const double qr = 1.0 - ger, qi = -gei;
-    const double iq = 1.0 / (qr * qr + qi * qi);
-    const double Dr = C.v0s * (pr * qr + pim * qi) * iq;
-    const double Di = C.v0s * (pim * qr - pr * qi) * iq;
-    // C = kappa theta / sigma^2 * ((xi - d) T - 2 Log A)
-    const double Cr = C.kts * (amr * C.t - 2.0 * lr);
-    const double Ci = C.kts * (ami * C.t - 2.0 * li);
-    // i r phi T = (-rT*phi_im, rT*u);  i u x;  minus Log CF(-i)
-    double zre = Cr + Dr - C.rt * C.phi_im + C.lnm_re;
-    double zim = Ci + Di + C.rt * u + u * C.x + C.lnm_im;
+    const double iq = rcp_nr(fma(qr, qr, qi * qi));
+    const double Dr = fma(pr, qr, pim * qi) * iq;
+    const double Di = fma(pim, qr, -pr * qi) * iq;
+    // Ch = (xi - d) T - 2 Log A
+    const double Cr = fma(amr, C.t, -2.0 * lr);
+    const double Ci = fma(ami, C.t, -2.0 * li);
+    double zre = fma(C.kts, Cr, fma(C.v0s, Dr, C.z0re));
+    double zim = fma(C.kts, Ci, fma(C.v0s, Di, fma(C.rtx, u, C.z0im)));
     if (BATES) {
-        // J = lambda T (exp(i phi mu_j - phi^2 sigma_j^2/2) - 1 - i phi comp)
-        const double jr_in = -C.phi_im * C.mu_j - C.hs2 * (u * u - C.phi_im * C.phi_im);
-        const double ji_in = u * C.mu_j - C.hs2 * (2.0 * u * C.phi_im);
         double js, jc;
-        sincos(ji_in, &js, &jc);
-        const double je = exp(jr_in);
-        zre += C.lt * (je * jc - 1.0 + C.phi_im * C.comp);
-        zim += C.lt * (je * js - u * C.comp);
+        sincos(C.jmu * u, &js, &jc);
+        const double je = C.lt * exp(fma(-C.hs2, u2, C.jr0));
+        zre += fma(je, jc, C.jre0);
+        zim += fma(je, js, -C.ltc * u);
     }
-    const double v = (exp(zre) * sin(zim) / u) / (tn * tn);
+    // Im(e^Z) / u / t^2 = e^{Re Z} sin(Im Z) / ((1 - t) t)
+    const double v = exp(zre) * sin(zim) * rcp_nr(omt * tn);
     const bool ok = (tn > 0.0) && (u >= 1e-12) && isfinite(v);
     return ok ? v : 0.0;
 }

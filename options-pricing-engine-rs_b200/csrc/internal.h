@@ -66,8 +66,15 @@ PriceScratch carve_price_scratch(void* base, size_t n);
 int launch_price_persistent(int model, const ope_contract* con, size_t n, const int64_t* surf_offsets,
                             size_t n_surf, const int32_t* param_idx, const double* params, double tol, double* out,
                             const PriceScratch& s, cudaStream_t st, int32_t* nbis_out = nullptr);
+// Price + reverse-mode parameter gradient (adjoint.cu); `scratch` must hold
+// grad_scratch_bytes(n, dim) bytes; out_grad is n x dim (dim 5 or 8).
+size_t grad_scratch_bytes(size_t n, int dim);
+int launch_price_grad(int model, const ope_contract* con, size_t n, const int64_t* surf_offsets, size_t n_surf,
+                      const int32_t* param_idx, const double* params, double tol, double* out_price,
+                      double* out_grad, void* scratch, cudaStream_t st);
 // DFMA throughput probe: FP64 flop/s (2 per FMA) over ~`ms_target` ms.
 int measure_fp64_peak(double* flops, double* ms);
+int selftest_math(uint64_t* ulp_rcp, uint64_t* ulp_sqrt);
 // Bump-and-reprice Greeks (greeks.rs:19-72) for n contracts under one
 // parameter set; `ws` must hold greeks_workspace_bytes(n) bytes.
 size_t greeks_workspace_bytes(size_t n);

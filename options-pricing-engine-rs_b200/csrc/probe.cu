@@ -7,6 +7,7 @@
 // warps per SM, timed with CUDA events.  Counted as 2 flops per DFMA.
 #include <cuda_runtime.h>
 
+#include "cf_device.cuh"
 #include "internal.h"
 
 namespace ope {
@@ -23,7 +24,44 @@ __global__ void __launch_bounds__(256) k_dfma_probe(double b, double c, int iter
     if (s == 1234.5678) sink[0] = s;  // never true; keeps the chains live
 }
 
+// rcp_nr / rsqrt_nr against IEEE 1/x and sqrt over 2^20 inputs spanning
+// 1e-300 .. 1e300 (log-uniform exponent, pseudo-random mantissa).  Errors in
+// units of the last place of the correctly rounded result.
+__global__ void k_selftest_math(unsigned long long* ulp_rcp, unsigned long long* ulp_sqrt) {
+    const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long h = 0x9E3779B97F4A7C15ull * (i + 1);
+    h ^= h >> 31;
+    h *= 0xBF58476D1CE4E5B9ull;
+    h ^= h >> 29;
+    const double mant = 1.0 + (double)(h >> 12) * 0x1.0p-52;
+    const double ex = -996.0 + 1992.0 * ((double)(i & 0xffff) / 65535.0);
+    const double x = ldexp(mant, (int)ex);
+    const double a = rcp_nr(x), b = 1.0 / x;
+    const long long da = llabs(__double_as_longlong(a) - __double_as_longlong(b));
+    const double s = x * rsqrt_nr(x), t = sqrt(x);
+    const long long ds = llabs(__double_as_longlong(s) - __double_as_longlong(t));
+    atomicMax(ulp_rcp, (unsigned long long)da);
+    atomicMax(ulp_sqrt, (unsigned long long)ds);
+}
+
 }  // namespace
+
+int selftest_math(uint64_t* ulp_rcp, uint64_t* ulp_sqrt) {
+    ThreadCtx& c = tctx();
+    void* ws;
+    OPE_TRY(ensure_workspace(256, &ws));
+    unsigned long long* d = static_cast<unsigned long long*>(ws);
+    OPE_CHECK(cudaMemsetAsync(d, 0, 2 * sizeof(unsigned long long), c.stream));
+    k_selftest_math<<<4096, 256, 0, c.stream>>>(d, d + 1);
+    OPE_CHECK(cudaGetLastError());
+    c.launches += 1;
+    unsigned long long h[2];
+    OPE_CHECK(cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, c.stream));
+    OPE_CHECK(cudaStreamSynchronize(c.stream));
+    *ulp_rcp = h[0];
+    *ulp_sqrt = h[1];
+    return OPE_OK;
+}
 
 int measure_fp64_peak(double* flops, double* ms) {
     ThreadCtx& c = tctx();

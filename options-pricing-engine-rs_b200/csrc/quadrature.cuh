@@ -30,7 +30,7 @@ constexpr int kMaxPanels = 200;  // heston.rs:194
 // GK15 nodes and weights in the reference's order (heston.rs:29-49) with a
 // zero pad at index 15, and the G7 weight scattered onto its Kronrod index
 // (G7_IDX = {0,3,4,7,8,11,12}, heston.rs:53-59), zero elsewhere.
-__constant__ double c_gk_x[16] = {
+static __constant__ double c_gk_x[16] = {
     0.0,
     0.2077849550078985, -0.2077849550078985,
     0.4058451513773972, -0.4058451513773972,
@@ -40,7 +40,7 @@ __constant__ double c_gk_x[16] = {
     0.9491079123427585, -0.9491079123427585,
     0.9914553711208126, -0.9914553711208126,
     0.0};
-__constant__ double c_gk_wk[16] = {
+static __constant__ double c_gk_wk[16] = {
     0.2094821410847278,
     0.2044329400752989, 0.2044329400752989,
     0.1903505780647854, 0.1903505780647854,
@@ -50,7 +50,7 @@ __constant__ double c_gk_wk[16] = {
     0.0630920926299786, 0.0630920926299786,
     0.0229353220105292, 0.0229353220105292,
     0.0};
-__constant__ double c_gk_wg[16] = {
+static __constant__ double c_gk_wg[16] = {
     0.4179591836734694,
     0.0, 0.0,
     0.3818300505051189, 0.3818300505051189,
@@ -96,35 +96,76 @@ __device__ __forceinline__ void half_warp_sum2(double& a, double& b) {
 }
 
 // Returns the integral (identical in every lane).  `nbis` receives the
-// number of bisections (loop iterations of heston.rs:200-210).
+// number of bisections (loop iterations of heston.rs:200-210); the final
+// live-panel list (nbis + 1 entries) is left in L.  The first panel and every
+// bisection go through ONE call site of the integrand, so the (large) inlined
+// node evaluation exists once in the instruction stream.
 template <bool BATES>
 __device__ __forceinline__ double gk_integrate_warp(const CfConsts& C, double tol, PanelStore& L, int lane,
                                                     const LaneRule& R, int* nbis) {
     const unsigned FULL = 0xffffffffu;
-    // First panel [0, 1]: c = h = 0.5; only the left half-warp has nodes.
-    double f = 0.0;
-    if (R.half == 0 && R.node) f = node_value<BATES>(C, __dadd_rn(0.5, __dmul_rn(0.5, R.x)));
-    double ks = R.wk * f, gs = R.wg * f;
-    half_warp_sum2(ks, gs);
-    const double K0 = __shfl_sync(FULL, ks, 0), G0 = __shfl_sync(FULL, gs, 0);
-    const double k0 = __dmul_rn(K0, 0.5);
-    const double e0 = __dmul_rn(fabs(K0 - G0), 0.5);
-    if (lane == 0) {
-        L.ekey[0] = (unsigned long long)__double_as_longlong(e0);
-        L.k[0] = k0;
-        L.a[0] = 0.0;
-        L.b[0] = 1.0;
-    }
-    __syncwarp();
-    double total = k0, err = e0;
-    int len = 1, nb = 0;
-    while (err > tol && len < kMaxPanels) {
+    double total = 0.0, err = 0.0;
+    int len = 0;
+    // panel under evaluation in this half-warp; first step: [0, 1] on the left half only
+    double pa = 0.0, pb = 1.0;
+    bool active = (R.half == 0) && R.node;
+    double aw = 0.0, bw = 1.0, m = 0.5, kw = 0.0, ew = 0.0;
+    int w = 0;
+    while (true) {
+        const double c = 0.5 * (pa + pb), h = 0.5 * (pb - pa);
+        const double f = active ? node_value<BATES>(C, __dadd_rn(c, __dmul_rn(h, R.x))) : 0.0;
+        double ks = R.wk * f, gs = R.wg * f;
+        half_warp_sum2(ks, gs);
+        const double Kl = __shfl_sync(FULL, ks, 0), Gl = __shfl_sync(FULL, gs, 0);
+        const double Kr = __shfl_sync(FULL, ks, 16), Gr = __shfl_sync(FULL, gs, 16);
+        if (len == 0) {
+            const double k0 = __dmul_rn(Kl, 0.5), e0 = __dmul_rn(fabs(Kl - Gl), 0.5);
+            if (lane == 0) {
+                L.ekey[0] = (unsigned long long)__double_as_longlong(e0);
+                L.k[0] = k0;
+                L.a[0] = 0.0;
+                L.b[0] = 1.0;
+            }
+            total = k0;
+            err = e0;
+            len = 1;
+        } else {
+            const double hl = 0.5 * (m - aw), hr = 0.5 * (bw - m);
+            const double kl = __dmul_rn(Kl, hl), el = __dmul_rn(fabs(Kl - Gl), hl);
+            const double kr = __dmul_rn(Kr, hr), er = __dmul_rn(fabs(Kr - Gr), hr);
+            total = __dadd_rn(total, __dsub_rn(__dadd_rn(kl, kr), kw));
+            err = __dadd_rn(err, __dsub_rn(__dadd_rn(el, er), ew));
+            if (lane == 0) {
+                const int last = len - 1;
+                if (w != last) {  // swap_remove
+                    L.ekey[w] = L.ekey[last];
+                    L.k[w] = L.k[last];
+                    L.a[w] = L.a[last];
+                    L.b[w] = L.b[last];
+                }
+                L.ekey[last] = (unsigned long long)__double_as_longlong(el);
+                L.k[last] = kl;
+                L.a[last] = aw;
+                L.b[last] = m;
+                L.ekey[len] = (unsigned long long)__double_as_longlong(er);
+                L.k[len] = kr;
+                L.a[len] = m;
+                L.b[len] = bw;
+            }
+            ++len;
+        }
+        __syncwarp();
+        if (!(err > tol && len < kMaxPanels)) break;
         // argmax over the live list, last maximum wins (Iterator::max_by).
         unsigned long long best = 0ull;
         int bi = -1;
-        for (int i = lane; i < len; i += 32) {
-            const unsigned long long kk = L.ekey[i];
-            if (kk >= best) { best = kk; bi = i; }
+#pragma unroll
+        for (int j = 0; j < (kMaxPanels + 31) / 32; ++j) {
+            const int i = lane + 32 * j;
+            if (i < len) {
+                const unsigned long long kk = L.ekey[i];
+                if (kk >= best) { best = kk; bi = i; }
+            }
         }
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) {
@@ -132,46 +173,18 @@ __device__ __forceinline__ double gk_integrate_warp(const CfConsts& C, double to
             const int oi = __shfl_xor_sync(FULL, bi, off);
             if (ob > best || (ob == best && oi > bi)) { best = ob; bi = oi; }
         }
-        const int w = bi;
-        const double ew = __longlong_as_double((long long)best);
-        const double kw = L.k[w], aw = L.a[w], bw = L.b[w];
-        const double m = 0.5 * (aw + bw);
-        const double pa = R.half ? m : aw, pb = R.half ? bw : m;
-        const double c = 0.5 * (pa + pb), h = 0.5 * (pb - pa);
-        f = R.node ? node_value<BATES>(C, __dadd_rn(c, __dmul_rn(h, R.x))) : 0.0;
-        ks = R.wk * f;
-        gs = R.wg * f;
-        half_warp_sum2(ks, gs);
-        const double Kl = __shfl_sync(FULL, ks, 0), Gl = __shfl_sync(FULL, gs, 0);
-        const double Kr = __shfl_sync(FULL, ks, 16), Gr = __shfl_sync(FULL, gs, 16);
-        const double hl = 0.5 * (m - aw), hr = 0.5 * (bw - m);
-        const double kl = __dmul_rn(Kl, hl), el = __dmul_rn(fabs(Kl - Gl), hl);
-        const double kr = __dmul_rn(Kr, hr), er = __dmul_rn(fabs(Kr - Gr), hr);
-        total = __dadd_rn(total, __dsub_rn(__dadd_rn(kl, kr), kw));
-        err = __dadd_rn(err, __dsub_rn(__dadd_rn(el, er), ew));
-        __syncwarp();  // every lane has read entry w
-        if (lane == 0) {
-            const int last = len - 1;
-            if (w != last) {  // swap_remove
-                L.ekey[w] = L.ekey[last];
-                L.k[w] = L.k[last];
-                L.a[w] = L.a[last];
-                L.b[w] = L.b[last];
-            }
-            L.ekey[last] = (unsigned long long)__double_as_longlong(el);
-            L.k[last] = kl;
-            L.a[last] = aw;
-            L.b[last] = m;
-            L.ekey[len] = (unsigned long long)__double_as_longlong(er);
-            L.k[len] = kr;
-            L.a[len] = m;
-            L.b[len] = bw;
-        }
-        __syncwarp();
-        ++len;
-        ++nb;
+        w = bi;
+        ew = __longlong_as_double((long long)best);
+        kw = L.k[w];
+        aw = L.a[w];
+        bw = L.b[w];
+        m = 0.5 * (aw + bw);
+        pa = R.half ? m : aw;
+        pb = R.half ? bw : m;
+        active = R.node;
+        __syncwarp();  // every lane has read entry w before lane 0 rewrites it
     }
-    *nbis = nb;
+    *nbis = len - 1;
     return total;
 }
 

@@ -201,6 +201,29 @@ def price_surfaces(model: int, contracts, surf_offsets, params, tol=REF_TOL, out
     return out
 
 
+def price_gradient_surfaces(model: int, contracts, surf_offsets, params, tol=REF_TOL):
+    """Prices and d price / d params (n x 5 Heston, n x 8 Bates) by the adjoint kernel.
+
+    The parameter order is (v0, kappa, theta, sigma, rho[, lambda, mu_j, sigma_j]);
+    the same derivatives ad.rs:695-731 / 882-895 compute by forward-mode AD.
+    """
+    con = contracts_array(contracts)
+    off = np.ascontiguousarray(surf_offsets, dtype=np.int64)
+    p = _params_array(params, model)
+    n_surf = off.size - 1
+    if p.ndim != 2 or p.shape[0] != n_surf:
+        raise ValueError("params must be (n_surf, 5|8)")
+    dim = p.shape[1]
+    price = np.empty(con.size, dtype=np.float64)
+    grad = np.empty((con.size, dim), dtype=np.float64)
+    if con.size == 0:
+        return price, grad
+    o = _opts(tol)
+    check(load().ope_price_gradient_surfaces(model, con.ctypes.data, con.size, off.ctypes.data, n_surf,
+                                             p.ctypes.data, price.ctypes.data, grad.ctypes.data, ctypes.byref(o)))
+    return price, grad
+
+
 def measure_fp64_peak() -> tuple[float, float]:
     """(flop/s, ms) of the DFMA throughput probe on the current device."""
     f, ms = ctypes.c_double(), ctypes.c_double()
@@ -246,5 +269,5 @@ __all__ = [
     "OptionType", "OptionContract", "HestonParams", "BatesParams", "PricingResult", "OpeError",
     "heston_price", "bates_price", "batch_heston", "batch_bates", "batch_heston_greeks", "batch_bates_greeks",
     "price_surfaces", "price_surfaces_device", "batch_price_device", "contracts_array", "REF_TOL",
-    "MODEL_HESTON", "MODEL_BATES", "RESULT_DTYPE", "kernel_launch_count", "device_info", "measure_fp64_peak",
+    "MODEL_HESTON", "MODEL_BATES", "RESULT_DTYPE", "kernel_launch_count", "device_info", "measure_fp64_peak", "price_gradient_surfaces",
 ]

@@ -275,3 +275,13 @@ def test_full_c3_properties_and_determinism(ope, oracle):
     seg = a[w.surf_offsets[s]:w.surf_offsets[s + 1]]
     assert np.array_equal(alone, seg)
     assert np.array_equal(ope.batch_bates(sub.contracts, sub.params[0], tol=w.tol), seg)
+
+
+def test_newton_reciprocal_and_sqrt_within_two_ulp(ope):
+    import ctypes
+
+    from ope_b200 import _lib
+
+    a, b = ctypes.c_uint64(), ctypes.c_uint64()
+    _lib.check(_lib.load().ope_selftest_math(ctypes.byref(a), ctypes.byref(b)))
+    assert a.value <= 2 and b.value <= 2, (a.value, b.value)
