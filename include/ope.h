@@ -77,6 +77,16 @@ typedef struct {
     double price, delta, gamma, vega, theta, rho, vanna, volga;
 } ope_pricing_result;
 
+/* calibration.rs:44-68 CalibResult.  params holds (v0, kappa, theta, sigma,
+ * rho[, lambda, mu_j, sigma_j]); status: 1 converged (gradient or step
+ * test), 2 stopped on the damping cap, 3 stopped on the iteration cap. */
+typedef struct {
+    double params[8];
+    double rmse, max_err, condition_number;
+    double weakest_direction[8];
+    int32_t iters, converged, early_stopped, status;
+} ope_calib_result;
+
 typedef struct {
     double tol;        /* absolute GK15 tolerance; <= 0 selects OPE_REF_TOL */
     uint32_t flags;    /* OPE_FLAG_DEVICE_PTRS */
@@ -138,6 +148,28 @@ int ope_batch_greeks_ex(int32_t model, const ope_contract* contracts, size_t n, 
 int ope_price_surfaces(int32_t model, const ope_contract* contracts, size_t n,
                        const int64_t* surf_offsets, size_t n_surf, const void* params,
                        double* out_prices, const ope_options* opts);
+
+/* calibration.rs:204-210 calibrate_heston / calibrate_bates (calibrate_inner,
+ * calibration.rs:433-569), for many independent quote surfaces at once:
+ * Levenberg-Marquardt in implied-vol space, one state machine per surface,
+ * Jacobian from the adjoint kernel (d price/d p / BSM vega), the whole
+ * iteration loop run on the device as one CUDA graph (conditional WHILE).
+ * Surface s owns quotes [surf_offsets[s], surf_offsets[s+1]); iv_market[i]
+ * is quote i's market IV; weights may be NULL (all 1.0); p0 is n_surf x dim.
+ * out receives n_surf results.  Pricing tolerance: opts->tol (default 1e-8,
+ * the tolerance the reference calibrates with). */
+int ope_calibrate_surfaces(int32_t model, const ope_contract* quotes, const double* iv_market,
+                           const double* weights, size_t n_quotes, const int64_t* surf_offsets,
+                           size_t n_surf, const double* p0, ope_calib_result* out,
+                           const ope_options* opts);
+
+/* calibration.rs:613-652 jacobian (host pointers): the IV-space Jacobian the
+ * device LM uses, d iv_i / d p = (d price_i / d p) / vega_BSM(iv_i), rows of
+ * dim doubles, and the IV residuals iv_i - iv_market_i (out_res may be NULL),
+ * at params (n_surf x dim). */
+int ope_calib_jacobian(int32_t model, const ope_contract* quotes, const double* iv_market, size_t n_quotes,
+                       const int64_t* surf_offsets, size_t n_surf, const double* params, double* out_jac,
+                       double* out_res, const ope_options* opts);
 
 /* ad.rs:695-731 forward_pass (all parameters at once) / ad.rs:882-895
  * bates_jump_sensitivities_ad, batched over surfaces like ope_price_surfaces:

@@ -45,6 +45,7 @@ template <bool BATES>
 __global__ void __launch_bounds__(128) k_price_grad(const ope_contract* __restrict__ con, long long n,
                                                     const int64_t* __restrict__ surf_off, long long n_surf,
                                                     const int32_t* __restrict__ param_idx,
+                                                    const int32_t* __restrict__ surf_mask,
                                                     const double* __restrict__ params, double tol,
                                                     double* __restrict__ out_price, double* __restrict__ out_grad,
                                                     double* integ, double* ginteg, unsigned int* done,
@@ -64,6 +65,7 @@ __global__ void __launch_bounds__(128) k_price_grad(const ope_contract* __restri
         const int which = (int)(unit & 1);
         const long long s = param_idx ? (long long)__ldg(param_idx + c)
                                       : (n_surf > 1 ? find_surface_g(surf_off, n_surf, c) : 0);
+        if (surf_mask && __ldg(surf_mask + s) == 0) continue;
         const double* p = params + s * DIM;
         double pl[8];
 #pragma unroll
@@ -151,7 +153,7 @@ size_t grad_scratch_bytes(size_t n, int dim) {
 
 int launch_price_grad(int model, const ope_contract* con, size_t n, const int64_t* surf_offsets, size_t n_surf,
                       const int32_t* param_idx, const double* params, double tol, double* out_price,
-                      double* out_grad, void* scratch, cudaStream_t st) {
+                      double* out_grad, void* scratch, cudaStream_t st, const int32_t* surf_mask) {
     if (n == 0) return OPE_OK;
     const PriceScratch s = carve_price_scratch(scratch, n);
     double* ginteg = reinterpret_cast<double*>(static_cast<char*>(scratch) + price_scratch_bytes(n));
@@ -163,11 +165,11 @@ int launch_price_grad(int model, const ope_contract* con, size_t n, const int64_
     if (model == OPE_MODEL_BATES) {
         OPE_TRY(grad_grid(k_price_grad<true>, smem, need, &grid));
         k_price_grad<true><<<grid, 128, smem, st>>>(con, (long long)n, surf_offsets, (long long)n_surf, param_idx,
-                                                    params, tol, out_price, out_grad, s.integ, ginteg, s.done, s.head);
+                                                    surf_mask, params, tol, out_price, out_grad, s.integ, ginteg, s.done, s.head);
     } else {
         OPE_TRY(grad_grid(k_price_grad<false>, smem, need, &grid));
         k_price_grad<false><<<grid, 128, smem, st>>>(con, (long long)n, surf_offsets, (long long)n_surf, param_idx,
-                                                     params, tol, out_price, out_grad, s.integ, ginteg, s.done, s.head);
+                                                     surf_mask, params, tol, out_price, out_grad, s.integ, ginteg, s.done, s.head);
     }
     OPE_CHECK(cudaGetLastError());
     tctx().launches += 1;

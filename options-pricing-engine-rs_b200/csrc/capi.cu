@@ -243,6 +243,36 @@ int ope_batch_greeks_ex(int32_t model, const ope_contract* contracts, size_t n, 
     return batch_greeks(model, contracts, n, params, out, opts);
 }
 
+int ope_calibrate_surfaces(int32_t model, const ope_contract* quotes, const double* iv_market, const double* weights,
+                           size_t n_quotes, const int64_t* surf_offsets, size_t n_surf, const double* p0,
+                           ope_calib_result* out, const ope_options* opts) {
+    OPE_TRY(check_model(model));
+    double tol;
+    OPE_TRY(resolve_tol(opts, &tol));
+    if (n_surf == 0) return OPE_OK;
+    if (!quotes || !iv_market || !surf_offsets || !p0 || !out) return set_error(OPE_ERR_INVALID_ARG, "NULL argument");
+    if (n_quotes == 0) return set_error(OPE_ERR_INVALID_ARG, "nothing to calibrate");  // calibration.rs:438
+    OPE_TRY(ensure_device());
+    return run_calibration(model, quotes, iv_market, weights, n_quotes, surf_offsets, n_surf, p0, out, tol,
+                           device_ptrs(opts), user_stream(opts));
+}
+
+int ope_calib_jacobian(int32_t model, const ope_contract* quotes, const double* iv_market, size_t n_quotes,
+                       const int64_t* surf_offsets, size_t n_surf, const double* params, double* out_jac,
+                       double* out_res, const ope_options* opts) {
+    OPE_TRY(check_model(model));
+    double tol;
+    OPE_TRY(resolve_tol(opts, &tol));
+    if (n_quotes == 0) return OPE_OK;
+    if (!quotes || !iv_market || !surf_offsets || !params || !out_jac || n_surf == 0)
+        return set_error(OPE_ERR_INVALID_ARG, "NULL argument");
+    if (device_ptrs(opts)) return set_error(OPE_ERR_INVALID_ARG, "ope_calib_jacobian takes host pointers");
+    if (surf_offsets[0] != 0 || surf_offsets[n_surf] != (int64_t)n_quotes)
+        return set_error(OPE_ERR_INVALID_ARG, "surf_offsets must span [0, n)");
+    OPE_TRY(ensure_device());
+    return run_calib_jacobian(model, quotes, iv_market, n_quotes, surf_offsets, n_surf, params, out_jac, out_res, tol);
+}
+
 int ope_price_gradient_surfaces(int32_t model, const ope_contract* contracts, size_t n, const int64_t* surf_offsets,
                                 size_t n_surf, const void* params, double* out_prices, double* out_grad,
                                 const ope_options* opts) {

@@ -62,16 +62,26 @@ PriceScratch carve_price_scratch(void* base, size_t n);
 // Device launchers (stream-ordered; all pointers are device pointers).
 // Contract c is priced with params + stride * p(c), where p(c) = param_idx[c]
 // when param_idx is non-NULL, else the surface of c under surf_offsets
-// (n_surf + 1 entries), else 0.
+// (n_surf + 1 entries), else 0.  With surf_mask non-NULL, units whose p(c)
+// has surf_mask[p(c)] == 0 are skipped (their outputs are left untouched).
 int launch_price_persistent(int model, const ope_contract* con, size_t n, const int64_t* surf_offsets,
                             size_t n_surf, const int32_t* param_idx, const double* params, double tol, double* out,
-                            const PriceScratch& s, cudaStream_t st, int32_t* nbis_out = nullptr);
+                            const PriceScratch& s, cudaStream_t st, int32_t* nbis_out = nullptr,
+                            const int32_t* surf_mask = nullptr);
 // Price + reverse-mode parameter gradient (adjoint.cu); `scratch` must hold
 // grad_scratch_bytes(n, dim) bytes; out_grad is n x dim (dim 5 or 8).
 size_t grad_scratch_bytes(size_t n, int dim);
 int launch_price_grad(int model, const ope_contract* con, size_t n, const int64_t* surf_offsets, size_t n_surf,
                       const int32_t* param_idx, const double* params, double tol, double* out_price,
-                      double* out_grad, void* scratch, cudaStream_t st);
+                      double* out_grad, void* scratch, cudaStream_t st, const int32_t* surf_mask = nullptr);
+// Batched LM calibration (calib.cu).
+size_t calib_workspace_bytes(size_t nq, size_t ns, int dim);
+int run_calibration(int model, const ope_contract* quotes, const double* iv_market, const double* weights, size_t nq,
+                    const int64_t* surf_offsets, size_t ns, const double* p0, ope_calib_result* out, double tol,
+                    bool device_ptrs, cudaStream_t st);
+int run_calib_jacobian(int model, const ope_contract* quotes, const double* iv_market, size_t nq,
+                       const int64_t* surf_offsets, size_t ns, const double* params, double* out_jac,
+                       double* out_res, double tol);
 // DFMA throughput probe: FP64 flop/s (2 per FMA) over ~`ms_target` ms.
 int measure_fp64_peak(double* flops, double* ms);
 int selftest_math(uint64_t* ulp_rcp, uint64_t* ulp_sqrt);

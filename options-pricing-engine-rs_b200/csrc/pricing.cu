@@ -23,7 +23,7 @@
 #define OPE_KERNEL_WARPS 4
 #endif
 #ifndef OPE_KERNEL_MINB
-#define OPE_KERNEL_MINB 1
+#define OPE_KERNEL_MINB 6
 #endif
 
 namespace ope {
@@ -106,6 +106,7 @@ template <bool BATES>
 __global__ void __launch_bounds__(OPE_KERNEL_WARPS * 32, OPE_KERNEL_MINB) k_price_persistent(const ope_contract* __restrict__ con, long long n,
                                                           const int64_t* __restrict__ surf_off, long long n_surf,
                                                           const int32_t* __restrict__ param_idx,
+                                                          const int32_t* __restrict__ surf_mask,
                                                           const double* __restrict__ params, double tol,
                                                           double* __restrict__ out, double* integ,
                                                           unsigned int* done, unsigned long long* head,
@@ -123,6 +124,7 @@ __global__ void __launch_bounds__(OPE_KERNEL_WARPS * 32, OPE_KERNEL_MINB) k_pric
         const long long c = (long long)(unit >> 1);
         const long long s = param_idx ? (long long)__ldg(param_idx + c)
                                       : (n_surf > 1 ? find_surface(surf_off, n_surf, c) : 0);
+        if (surf_mask && __ldg(surf_mask + s) == 0) continue;
         run_unit<BATES>(c, (int)(unit & 1), con, params + s * stride, tol, out, integ, done, nbis_out,
                         smem_panels[warp], lane, R);
     }
@@ -142,7 +144,7 @@ int persistent_grid(K kernel, int threads, size_t smem, int* grid) {
 
 int launch_price_persistent(int model, const ope_contract* con, size_t n, const int64_t* surf_offsets,
                             size_t n_surf, const int32_t* param_idx, const double* params, double tol, double* out,
-                            const PriceScratch& s, cudaStream_t st, int32_t* nbis_out) {
+                            const PriceScratch& s, cudaStream_t st, int32_t* nbis_out, const int32_t* surf_mask) {
     if (n == 0) return OPE_OK;
     OPE_CHECK(cudaMemsetAsync(s.done, 0, n * sizeof(unsigned int), st));
     OPE_CHECK(cudaMemsetAsync(s.head, 0, sizeof(unsigned long long), st));
@@ -154,13 +156,13 @@ int launch_price_persistent(int model, const ope_contract* con, size_t n, const 
         const unsigned long long need = (2ull * n + warps - 1) / warps;
         grid = (int)std::min<unsigned long long>((unsigned long long)grid, need);
         k_price_persistent<true><<<grid, threads, smem, st>>>(con, (long long)n, surf_offsets, (long long)n_surf,
-                                                              param_idx, params, tol, out, s.integ, s.done, s.head, nbis_out);
+                                                              param_idx, surf_mask, params, tol, out, s.integ, s.done, s.head, nbis_out);
     } else {
         OPE_TRY(persistent_grid(k_price_persistent<false>, threads, smem, &grid));
         const unsigned long long need = (2ull * n + warps - 1) / warps;
         grid = (int)std::min<unsigned long long>((unsigned long long)grid, need);
         k_price_persistent<false><<<grid, threads, smem, st>>>(con, (long long)n, surf_offsets, (long long)n_surf,
-                                                               param_idx, params, tol, out, s.integ, s.done, s.head, nbis_out);
+                                                               param_idx, surf_mask, params, tol, out, s.integ, s.done, s.head, nbis_out);
     }
     OPE_CHECK(cudaGetLastError());
     tctx().launches += 1;

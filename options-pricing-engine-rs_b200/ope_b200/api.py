@@ -224,6 +224,64 @@ def price_gradient_surfaces(model: int, contracts, surf_offsets, params, tol=REF
     return price, grad
 
 
+CALIB_RESULT_DTYPE = np.dtype([
+    ("params", "<f8", (8,)), ("rmse", "<f8"), ("max_err", "<f8"), ("condition_number", "<f8"),
+    ("weakest_direction", "<f8", (8,)), ("iters", "<i4"), ("converged", "<i4"), ("early_stopped", "<i4"),
+    ("status", "<i4"),
+])  # include/ope.h ope_calib_result = calibration.rs:44-68 CalibResult
+
+
+def calibrate_surfaces(model: int, quotes, iv_market, surf_offsets, p0, weights=None, tol=REF_TOL) -> np.ndarray:
+    """Levenberg-Marquardt in IV space for many quote surfaces at once (calibration.rs:433-569).
+
+    Returns one CALIB_RESULT_DTYPE record per surface; ``params[:dim]`` are the fitted
+    (v0, kappa, theta, sigma, rho[, lambda, mu_j, sigma_j]).
+    """
+    con = contracts_array(quotes)
+    iv = np.ascontiguousarray(iv_market, dtype=np.float64)
+    off = np.ascontiguousarray(surf_offsets, dtype=np.int64)
+    p = _params_array(p0, model)
+    n_surf = off.size - 1
+    if p.ndim != 2 or p.shape[0] != n_surf:
+        raise ValueError("p0 must be (n_surf, 5|8)")
+    if iv.size != con.size:
+        raise ValueError("iv_market must have one entry per quote")
+    w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+    out = np.zeros(n_surf, dtype=CALIB_RESULT_DTYPE)
+    o = _opts(tol)
+    check(load().ope_calibrate_surfaces(model, con.ctypes.data, iv.ctypes.data, None if w is None else w.ctypes.data,
+                                        con.size, off.ctypes.data, n_surf, p.ctypes.data, out.ctypes.data,
+                                        ctypes.byref(o)))
+    return out
+
+
+def calibrate_heston(quotes, iv_market, p0, weights=None, tol=REF_TOL):
+    """calibration.rs:204-206 (one surface)."""
+    return calibrate_surfaces(MODEL_HESTON, quotes, iv_market, [0, len(iv_market)], np.atleast_2d(
+        _params_array(p0, MODEL_HESTON)), weights, tol)[0]
+
+
+def calibrate_bates(quotes, iv_market, p0, weights=None, tol=REF_TOL):
+    """calibration.rs:208-210 (one surface)."""
+    return calibrate_surfaces(MODEL_BATES, quotes, iv_market, [0, len(iv_market)], np.atleast_2d(
+        _params_array(p0, MODEL_BATES)), weights, tol)[0]
+
+
+def calib_jacobian(model: int, quotes, iv_market, surf_offsets, params, tol=REF_TOL):
+    """The device IV-space Jacobian (n x dim) and IV residuals at params (calibration.rs:613-652)."""
+    con = contracts_array(quotes)
+    iv = np.ascontiguousarray(iv_market, dtype=np.float64)
+    off = np.ascontiguousarray(surf_offsets, dtype=np.int64)
+    p = _params_array(params, model)
+    dim = p.shape[-1]
+    jac = np.zeros((con.size, dim))
+    res = np.zeros(con.size)
+    o = _opts(tol)
+    check(load().ope_calib_jacobian(model, con.ctypes.data, iv.ctypes.data, con.size, off.ctypes.data, off.size - 1,
+                                    p.ctypes.data, jac.ctypes.data, res.ctypes.data, ctypes.byref(o)))
+    return jac, res
+
+
 def measure_fp64_peak() -> tuple[float, float]:
     """(flop/s, ms) of the DFMA throughput probe on the current device."""
     f, ms = ctypes.c_double(), ctypes.c_double()
@@ -270,4 +328,5 @@ __all__ = [
     "heston_price", "bates_price", "batch_heston", "batch_bates", "batch_heston_greeks", "batch_bates_greeks",
     "price_surfaces", "price_surfaces_device", "batch_price_device", "contracts_array", "REF_TOL",
     "MODEL_HESTON", "MODEL_BATES", "RESULT_DTYPE", "kernel_launch_count", "device_info", "measure_fp64_peak", "price_gradient_surfaces",
+    "CALIB_RESULT_DTYPE", "calibrate_surfaces", "calibrate_heston", "calibrate_bates", "calib_jacobian",
 ]

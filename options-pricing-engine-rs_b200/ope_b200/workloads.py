@@ -177,3 +177,28 @@ def c4_grid(n_surf: int = 256, n_k: int = 30, n_t: int = 10, seed: int = 4):
 
 def by_name(name: str) -> Workload:
     return {"c1": c1, "c2": c2, "c3": c3}[name]()
+
+
+def c4(price_fn, iv_fn, n_surf: int = 256, n_k: int = 30, n_t: int = 10, seed: int = 4, noise: float = 0.005):
+    """Config 4 calibration problems: quotes priced from seeded true Heston
+    parameters (Feller-satisfying draws from the c2 ranges), inverted to IV,
+    perturbed by N(0, noise) IV noise; start points truth x U(0.7, 1.3).
+
+    price_fn(contracts, params, surf_idx) -> prices; iv_fn(contracts, prices) -> (iv, ok).
+    Quotes whose model IV cannot be inverted or falls outside (0.01, 2) are
+    dropped, as the reference's quote builder does (calibration.rs:993-995).
+    Returns (quotes, iv_market, offsets, true_params, p0).
+    """
+    con, off, true_p, _, _ = c4_grid(n_surf, n_k, n_t, seed)
+    sidx = np.repeat(np.arange(n_surf, dtype=np.int32), np.diff(off))
+    px = price_fn(con, true_p, sidx)
+    iv, ok = iv_fn(con, px)
+    ok = ok & (iv > 0.01) & (iv < 2.0)
+    rng = np.random.default_rng(seed + 1000)
+    iv_mkt = np.maximum(iv + rng.normal(0.0, noise, iv.size), 1e-3)
+    keep = np.where(ok)[0]
+    counts = np.bincount(sidx[keep], minlength=n_surf)
+    new_off = np.zeros(n_surf + 1, np.int64)
+    new_off[1:] = np.cumsum(counts)
+    p0 = true_p * rng.uniform(0.7, 1.3, true_p.shape)
+    return con[keep], iv_mkt[keep], new_off, true_p, p0

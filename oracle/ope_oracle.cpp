@@ -1133,6 +1133,18 @@ void orc_bsm_price_and_greeks(const void* contract, double* out8) {
     Result8 r = bsm_price_and_greeks(*static_cast<const Contract*>(contract));
     std::memcpy(out8, &r, sizeof(r));
 }
+void orc_batch_implied_vol(const void* contracts, int64_t n, const double* prices, double* out, int32_t* ok,
+                           int nthreads) {
+    const Contract* c = static_cast<const Contract*>(contracts);
+    int nt = threads_or_default(nthreads);
+#pragma omp parallel for schedule(dynamic, 64) num_threads(nt)
+    for (int64_t i = 0; i < n; ++i) {
+        double v = 0.0;
+        ok[i] = implied_vol(c[i], prices[i], &v) ? 1 : 0;
+        out[i] = v;
+    }
+}
+
 int orc_implied_vol(const void* contract, double market_price, double* out) {
     return implied_vol(*static_cast<const Contract*>(contract), market_price, out) ? 1 : 0;
 }

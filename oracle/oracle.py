@@ -94,6 +94,7 @@ def lib() -> ctypes.CDLL:
             "orc_bsm_price": (d, [vp]),
             "orc_bsm_price_and_greeks": (None, [vp, dp]),
             "orc_implied_vol": (i, [vp, d, dp]),
+            "orc_batch_implied_vol": (None, [vp, i64, dp, dp, ip, i]),
             "orc_forward_pass": (None, [d, d, d, d, d, dp, i, i, i, d, d, d, i, d, dp, dp]),
             "orc_price_gradient": (None, [vp, dp, i, d, dp, dp]),
             "orc_batch_price_gradient": (None, [vp, i64, ip, dp, i, d, dp, dp, i]),
@@ -229,6 +230,16 @@ def implied_vol(c, market_price: float):
     out = np.zeros(1)
     ok = lib().orc_implied_vol(c.ctypes.data, float(market_price), _dptr(out))
     return float(out[0]) if ok else None
+
+
+def batch_implied_vol(con, prices, nthreads: int = 0):
+    """iv.rs:14-20 over many contracts: (iv, ok) arrays."""
+    con = np.ascontiguousarray(con, dtype=CONTRACT_DTYPE)
+    px = np.ascontiguousarray(prices, dtype=np.float64)
+    out = np.zeros(con.size)
+    ok = np.zeros(con.size, np.int32)
+    lib().orc_batch_implied_vol(con.ctypes.data, con.size, _dptr(px), _dptr(out), _iptr(ok), int(nthreads))
+    return out, ok.astype(bool)
 
 
 def forward_pass(s, k, t, r, q, hp, opt_type, active, jump=None, jump_active=-1, tol=REF_TOL):
