@@ -149,6 +149,12 @@ int ope_price_surfaces(int32_t model, const ope_contract* contracts, size_t n,
                        const int64_t* surf_offsets, size_t n_surf, const void* params,
                        double* out_prices, const ope_options* opts);
 
+/* batch.rs:51-56 batch_implied_vol (iv.rs:14-95 per contract): BSM implied
+ * volatility of market_prices[i] for contracts[i]; out_ok[i] = 0 where the
+ * reference returns None (out_iv[i] is then 0). */
+int ope_batch_implied_vol(const ope_contract* contracts, size_t n, const double* market_prices, double* out_iv,
+                          int32_t* out_ok, const ope_options* opts);
+
 /* calibration.rs:204-210 calibrate_heston / calibrate_bates (calibrate_inner,
  * calibration.rs:433-569), for many independent quote surfaces at once:
  * Levenberg-Marquardt in implied-vol space, one state machine per surface,
@@ -179,6 +185,53 @@ int ope_calib_jacobian(int32_t model, const ope_contract* quotes, const double* 
 int ope_price_gradient_surfaces(int32_t model, const ope_contract* contracts, size_t n,
                                 const int64_t* surf_offsets, size_t n_surf, const void* params,
                                 double* out_prices, double* out_grad, const ope_options* opts);
+
+/* ----------------------------------------------------------- serving */
+/* No reference twin (the reference is synchronous, batch.rs / calibration.rs):
+ * a device-resident request server with continuous batching.  Requests are
+ * queued by submit (non-blocking) and collected by wait.  A scheduler thread
+ * packs everything pending into micro-batches (one persistent pricing launch
+ * for reprices, one device-LM graph for calibrations) whenever a stream slot
+ * and device memory are free, so new requests are admitted while earlier ones
+ * are still running and their work overlaps on the GPU.  Admission is by
+ * device memory: the server reserves hbm_fraction of the FREE HBM at creation
+ * (capped by hbm_cap_bytes) and launches a batch when its buffers fit; a
+ * request that can never fit is rejected (OPE_ERR_REJECTED).  A request's
+ * results do not depend on what it was batched with. */
+typedef struct ope_server ope_server;
+
+typedef struct {
+    double tol;                    /* pricing tolerance; <= 0 selects OPE_REF_TOL */
+    double hbm_fraction;           /* share of free HBM to reserve (0 -> 0.5) */
+    uint64_t hbm_cap_bytes;        /* upper bound on that reservation (0 -> none) */
+    uint32_t max_inflight;         /* concurrent micro-batches = streams (0 -> 4) */
+    uint32_t max_batch_contracts;  /* contracts per micro-batch (0 -> 2^20) */
+    uint64_t pinned_bytes;         /* host staging (0 -> 256 MiB) */
+} ope_server_config;
+
+typedef struct {
+    uint64_t submitted, completed, rejected, cancelled, failed;
+    uint64_t batches, batched_requests, max_inflight;
+    uint64_t hbm_budget_bytes, hbm_peak_bytes, pending, inflight;
+} ope_server_stats;
+
+int ope_server_create(const ope_server_config* cfg, ope_server** out);
+int ope_server_destroy(ope_server* server);
+/* Reprice one surface: n contracts under one parameter set (batch.rs:23 / 38). */
+int ope_server_submit_price(ope_server* server, int32_t model, const ope_contract* contracts, size_t n,
+                            const void* params, uint64_t* out_id);
+/* Calibrate one quote surface from p0 (calibration.rs:204-210). */
+int ope_server_submit_calibrate(ope_server* server, int32_t model, const ope_contract* quotes,
+                                const double* iv_market, size_t n, const void* p0, uint64_t* out_id);
+/* Wait up to timeout_ms (< 0: forever) for a request; on OPE_OK the results go
+ * to out_prices (n doubles, reprice) or out_calib (calibration) and the
+ * request's latency (submit -> results on the host) to out_latency_ms.  The
+ * request is forgotten after a non-timeout return. */
+int ope_server_wait(ope_server* server, uint64_t id, double timeout_ms, double* out_prices,
+                    ope_calib_result* out_calib, double* out_latency_ms);
+/* Cancel a request that has not started yet. */
+int ope_server_cancel(ope_server* server, uint64_t id);
+int ope_server_get_stats(ope_server* server, ope_server_stats* out);
 
 /* ope_price_surfaces plus diagnostics: out_bisections (may be NULL) receives
  * 2n int32 — the bisection count of each contract's P1 and P2 integral (the

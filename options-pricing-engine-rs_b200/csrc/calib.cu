@@ -398,7 +398,15 @@ struct GraphCache {
     double tol = 0.0;
     cudaStream_t stream = nullptr;
 };
-thread_local GraphCache g_lm_graph;
+}  // namespace
+
+struct CalibGraph {
+    GraphCache cache;
+};
+
+namespace {
+
+thread_local CalibGraph g_lm_graph;
 
 struct Layout {
     size_t total;
@@ -522,58 +530,50 @@ int build_graph(int model, const LMDev& D, char* base, const Layout& L, double t
 
 size_t calib_workspace_bytes(size_t nq, size_t ns, int dim) { return layout(nq, ns, dim).total; }
 
-int run_calibration(int model, const ope_contract* quotes, const double* iv_market, const double* weights, size_t nq,
-                    const int64_t* surf_offsets, size_t ns, const double* p0, ope_calib_result* out, double tol,
-                    bool device_ptrs, cudaStream_t ust) {
+size_t calib_pinned_bytes(size_t nq, size_t ns, int dim) {
+    return align_up(nq * sizeof(int32_t), 256) + align_up(nq * sizeof(double), 256) +
+           align_up(ns * dim * sizeof(double), 256);
+}
+
+// Stage one calibration batch and enqueue all of it on `st`: inputs (kind:
+// host or device), the initial residual pass, the conditional-WHILE LM graph,
+// the final Jacobian and the diagnostics, and the copy of the results to
+// `out` (out_kind).  off_h is a host copy of the surface offsets; `pin` is a
+// pinned host buffer of calib_pinned_bytes(); `dev` a device region of
+// calib_workspace_bytes().  The graph is cached in *G when G->cache is set,
+// else it is left in *G for the caller to release after the stream completes.
+int calib_enqueue(int model, const ope_contract* quotes, const double* iv_market, const double* weights, size_t nq,
+                  const int64_t* surf_offsets, const int64_t* off_h, size_t ns, const double* p0,
+                  ope_calib_result* out, double tol, cudaMemcpyKind kind, cudaMemcpyKind out_kind, char* dev,
+                  char* pin, cudaStream_t st, CalibGraph* G) {
     ThreadCtx& c = tctx();
     const int dim = param_stride(model);
     const Layout L = layout(nq, ns, dim);
-    void* ws;
-    OPE_TRY(ensure_workspace(L.total, &ws));
-    char* base = static_cast<char*>(ws);
-    cudaStream_t st = device_ptrs ? ust : c.stream;
-    if (device_ptrs && st == nullptr) st = c.stream;  // capture needs a non-legacy stream
-    const cudaMemcpyKind kind = device_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-    // stage inputs
-    OPE_CHECK(cudaMemcpyAsync(base + L.q, quotes, nq * sizeof(ope_contract), kind, st));
-    OPE_CHECK(cudaMemcpyAsync(base + L.iv, iv_market, nq * sizeof(double), kind, st));
-    OPE_CHECK(cudaMemcpyAsync(base + L.off, surf_offsets, (ns + 1) * sizeof(int64_t), kind, st));
-    if (weights) {
-        OPE_CHECK(cudaMemcpyAsync(base + L.w, weights, nq * sizeof(double), kind, st));
-    }
-    // quote -> surface map and unit weights are built on the host (small)
-    std::vector<int64_t> off_h(ns + 1);
-    if (device_ptrs) {
-        OPE_CHECK(cudaMemcpyAsync(off_h.data(), surf_offsets, (ns + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-        OPE_CHECK(cudaStreamSynchronize(st));
-    } else {
-        std::memcpy(off_h.data(), surf_offsets, (ns + 1) * sizeof(int64_t));
-    }
+    char* base = dev;
     if (off_h[0] != 0 || off_h[ns] != (int64_t)nq) return set_error(OPE_ERR_INVALID_ARG, "surf_offsets must span [0, n)");
-    std::vector<int32_t> sidx(nq);
+    int32_t* sidx = reinterpret_cast<int32_t*>(pin);
     for (size_t s = 0; s < ns; ++s) {
         if (off_h[s + 1] < off_h[s]) return set_error(OPE_ERR_INVALID_ARG, "surf_offsets not sorted");
         for (int64_t i = off_h[s]; i < off_h[s + 1]; ++i) sidx[i] = (int32_t)s;
     }
-    void* pin;
-    const size_t pin_bytes = nq * sizeof(int32_t) + (weights ? 0 : nq * sizeof(double)) + ns * dim * sizeof(double);
-    OPE_TRY(ensure_pinned(pin_bytes, &pin));
-    char* ph = static_cast<char*>(pin);
-    std::memcpy(ph, sidx.data(), nq * sizeof(int32_t));
-    OPE_CHECK(cudaMemcpyAsync(base + L.sidx, ph, nq * sizeof(int32_t), cudaMemcpyHostToDevice, st));
-    char* ph2 = ph + nq * sizeof(int32_t);
-    if (!weights) {
-        double* wh = reinterpret_cast<double*>(ph2);
+    double* wh = reinterpret_cast<double*>(pin + align_up(nq * sizeof(int32_t), 256));
+    double* ph = reinterpret_cast<double*>(pin + align_up(nq * sizeof(int32_t), 256) + align_up(nq * sizeof(double), 256));
+    OPE_CHECK(cudaMemcpyAsync(base + L.q, quotes, nq * sizeof(ope_contract), kind, st));
+    OPE_CHECK(cudaMemcpyAsync(base + L.iv, iv_market, nq * sizeof(double), kind, st));
+    OPE_CHECK(cudaMemcpyAsync(base + L.off, surf_offsets, (ns + 1) * sizeof(int64_t), kind, st));
+    OPE_CHECK(cudaMemcpyAsync(base + L.sidx, sidx, nq * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+    if (weights) {
+        OPE_CHECK(cudaMemcpyAsync(base + L.w, weights, nq * sizeof(double), kind, st));
+    } else {
         for (size_t i = 0; i < nq; ++i) wh[i] = 1.0;
         OPE_CHECK(cudaMemcpyAsync(base + L.w, wh, nq * sizeof(double), cudaMemcpyHostToDevice, st));
-        ph2 += nq * sizeof(double);
     }
     const double* p0_dev;
-    if (device_ptrs) {
+    if (kind == cudaMemcpyDeviceToDevice) {
         p0_dev = p0;
     } else {
-        std::memcpy(ph2, p0, ns * dim * sizeof(double));
-        OPE_CHECK(cudaMemcpyAsync(base + L.ptrial, ph2, ns * dim * sizeof(double), cudaMemcpyHostToDevice, st));
+        std::memcpy(ph, p0, ns * dim * sizeof(double));
+        OPE_CHECK(cudaMemcpyAsync(base + L.ptrial, ph, ns * dim * sizeof(double), cudaMemcpyHostToDevice, st));
         p0_dev = reinterpret_cast<const double*>(base + L.ptrial);
     }
     LMDev D = make_dev(base, L, (int)nq, (int)ns, dim);
@@ -589,27 +589,87 @@ int run_calibration(int model, const ope_contract* quotes, const double* iv_mark
     OPE_CHECK(cudaMemsetAsync(D.counters, 0, 4 * sizeof(unsigned int), st));
     c.launches += 3;
     // the LM loop: one conditional-WHILE graph launch
-    GraphCache& G = g_lm_graph;
-    if (!(G.exec && G.ws == ws && G.model == model && G.nq == (int)nq && G.ns == (int)ns && G.tol == tol &&
-          G.stream == st)) {
-        OPE_TRY(build_graph(model, D, base, L, tol, st, G));
-        G.ws = ws;
-        G.model = model;
-        G.nq = (int)nq;
-        G.ns = (int)ns;
-        G.tol = tol;
-        G.stream = st;
+    GraphCache& g = G->cache;
+    if (!(g.exec && g.ws == dev && g.model == model && g.nq == (int)nq && g.ns == (int)ns && g.tol == tol &&
+          g.stream == st)) {
+        OPE_TRY(build_graph(model, D, base, L, tol, st, g));
+        g.ws = dev;
+        g.model = model;
+        g.nq = (int)nq;
+        g.ns = (int)ns;
+        g.tol = tol;
+        g.stream = st;
     }
-    OPE_CHECK(cudaGraphLaunch(G.exec, st));
+    OPE_CHECK(cudaGraphLaunch(g.exec, st));
     // final Jacobian at the last accepted parameters, diagnostics
     OPE_TRY(launch_jac(model, D, base, L, tol, st));
     ope_calib_result* d_out = reinterpret_cast<ope_calib_result*>(base + L.out);
     k_lm_final<<<((int)ns * 32 + 127) / 128, 128, 0, st>>>(D, d_out);
     OPE_CHECK(cudaGetLastError());
     c.launches += 1;
-    OPE_CHECK(cudaMemcpyAsync(out, d_out, ns * sizeof(ope_calib_result),
-                              device_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
-    if (!device_ptrs) OPE_CHECK(cudaStreamSynchronize(st));
+    OPE_CHECK(cudaMemcpyAsync(out, d_out, ns * sizeof(ope_calib_result), out_kind, st));
+    return OPE_OK;
+}
+
+CalibGraph* calib_graph_new() { return new CalibGraph(); }
+void calib_graph_delete(CalibGraph* G) {
+    if (!G) return;
+    calib_graph_release(G);
+    delete G;
+}
+
+void calib_graph_release(CalibGraph* G) {
+    GraphCache& g = G->cache;
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (g.graph) cudaGraphDestroy(g.graph);
+    g = GraphCache();
+}
+
+int run_calibration(int model, const ope_contract* quotes, const double* iv_market, const double* weights, size_t nq,
+                    const int64_t* surf_offsets, size_t ns, const double* p0, ope_calib_result* out, double tol,
+                    bool device_ptrs, cudaStream_t ust) {
+    ThreadCtx& c = tctx();
+    const int dim = param_stride(model);
+    void* ws;
+    OPE_TRY(ensure_workspace(calib_workspace_bytes(nq, ns, dim), &ws));
+    void* pin;
+    OPE_TRY(ensure_pinned(calib_pinned_bytes(nq, ns, dim), &pin));
+    cudaStream_t st = device_ptrs ? ust : c.stream;
+    if (device_ptrs && st == nullptr) st = c.stream;  // capture needs a non-legacy stream
+    std::vector<int64_t> off_h(ns + 1);
+    if (device_ptrs) {
+        OPE_CHECK(cudaMemcpyAsync(off_h.data(), surf_offsets, (ns + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+        OPE_CHECK(cudaStreamSynchronize(st));
+    } else {
+        std::memcpy(off_h.data(), surf_offsets, (ns + 1) * sizeof(int64_t));
+    }
+    const cudaMemcpyKind kind = device_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    OPE_TRY(calib_enqueue(model, quotes, iv_market, weights, nq, surf_offsets, off_h.data(), ns, p0, out, tol, kind,
+                          device_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, static_cast<char*>(ws),
+                          static_cast<char*>(pin), st, &g_lm_graph));
+    // the pinned staging is reused by the next call: wait for this one's copies
+    OPE_CHECK(cudaStreamSynchronize(st));
+    return OPE_OK;
+}
+
+namespace {
+// batch.rs:51-56 batch_implied_vol: one thread per contract.
+__global__ void k_batch_iv(const ope_contract* __restrict__ con, const double* __restrict__ price, long long n,
+                           double* __restrict__ iv, int32_t* __restrict__ ok) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double v = 0.0;
+    const bool good = implied_vol_d(iv_contract(con[i]), price[i], &v);
+    iv[i] = good ? v : 0.0;
+    ok[i] = good ? 1 : 0;
+}
+}  // namespace
+
+int launch_batch_iv(const ope_contract* con, const double* price, size_t n, double* iv, int32_t* ok, cudaStream_t st) {
+    if (n == 0) return OPE_OK;
+    k_batch_iv<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(con, price, (long long)n, iv, ok);
+    OPE_CHECK(cudaGetLastError());
+    tctx().launches += 1;
     return OPE_OK;
 }
 

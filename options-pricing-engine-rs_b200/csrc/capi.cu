@@ -243,6 +243,31 @@ int ope_batch_greeks_ex(int32_t model, const ope_contract* contracts, size_t n, 
     return batch_greeks(model, contracts, n, params, out, opts);
 }
 
+int ope_batch_implied_vol(const ope_contract* contracts, size_t n, const double* market_prices, double* out_iv,
+                          int32_t* out_ok, const ope_options* opts) {
+    if (n == 0) return OPE_OK;
+    if (!contracts || !market_prices || !out_iv || !out_ok) return set_error(OPE_ERR_INVALID_ARG, "NULL argument");
+    OPE_TRY(ensure_device());
+    if (device_ptrs(opts)) return launch_batch_iv(contracts, market_prices, n, out_iv, out_ok, user_stream(opts));
+    ThreadCtx& c = tctx();
+    const size_t b_con = align_up(n * sizeof(ope_contract), 256), b_d = align_up(n * sizeof(double), 256),
+                 b_i = align_up(n * sizeof(int32_t), 256);
+    void* ws;
+    OPE_TRY(ensure_workspace(b_con + 2 * b_d + b_i, &ws));
+    char* p = static_cast<char*>(ws);
+    ope_contract* d_con = reinterpret_cast<ope_contract*>(p);
+    double* d_px = reinterpret_cast<double*>(p + b_con);
+    double* d_iv = reinterpret_cast<double*>(p + b_con + b_d);
+    int32_t* d_ok = reinterpret_cast<int32_t*>(p + b_con + 2 * b_d);
+    OPE_CHECK(cudaMemcpyAsync(d_con, contracts, n * sizeof(ope_contract), cudaMemcpyHostToDevice, c.stream));
+    OPE_CHECK(cudaMemcpyAsync(d_px, market_prices, n * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    OPE_TRY(launch_batch_iv(d_con, d_px, n, d_iv, d_ok, c.stream));
+    OPE_CHECK(cudaMemcpyAsync(out_iv, d_iv, n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    OPE_CHECK(cudaMemcpyAsync(out_ok, d_ok, n * sizeof(int32_t), cudaMemcpyDeviceToHost, c.stream));
+    OPE_CHECK(cudaStreamSynchronize(c.stream));
+    return OPE_OK;
+}
+
 int ope_calibrate_surfaces(int32_t model, const ope_contract* quotes, const double* iv_market, const double* weights,
                            size_t n_quotes, const int64_t* surf_offsets, size_t n_surf, const double* p0,
                            ope_calib_result* out, const ope_options* opts) {

@@ -75,13 +75,24 @@ int launch_price_grad(int model, const ope_contract* con, size_t n, const int64_
                       const int32_t* param_idx, const double* params, double tol, double* out_price,
                       double* out_grad, void* scratch, cudaStream_t st, const int32_t* surf_mask = nullptr);
 // Batched LM calibration (calib.cu).
+struct CalibGraph;  // an instantiated LM graph (one per stream of use)
 size_t calib_workspace_bytes(size_t nq, size_t ns, int dim);
+size_t calib_pinned_bytes(size_t nq, size_t ns, int dim);
+int calib_enqueue(int model, const ope_contract* quotes, const double* iv_market, const double* weights, size_t nq,
+                  const int64_t* surf_offsets, const int64_t* off_h, size_t ns, const double* p0,
+                  ope_calib_result* out, double tol, cudaMemcpyKind kind, cudaMemcpyKind out_kind, char* dev,
+                  char* pin, cudaStream_t st, CalibGraph* G);
+CalibGraph* calib_graph_new();
+void calib_graph_release(CalibGraph* G);
+void calib_graph_delete(CalibGraph* G);
 int run_calibration(int model, const ope_contract* quotes, const double* iv_market, const double* weights, size_t nq,
                     const int64_t* surf_offsets, size_t ns, const double* p0, ope_calib_result* out, double tol,
                     bool device_ptrs, cudaStream_t st);
 int run_calib_jacobian(int model, const ope_contract* quotes, const double* iv_market, size_t nq,
                        const int64_t* surf_offsets, size_t ns, const double* params, double* out_jac,
                        double* out_res, double tol);
+// batch.rs:51-56 on the device (calib.cu).
+int launch_batch_iv(const ope_contract* con, const double* price, size_t n, double* iv, int32_t* ok, cudaStream_t st);
 // DFMA throughput probe: FP64 flop/s (2 per FMA) over ~`ms_target` ms.
 int measure_fp64_peak(double* flops, double* ms);
 int selftest_math(uint64_t* ulp_rcp, uint64_t* ulp_sqrt);

@@ -77,6 +77,14 @@ _sig("ope_selftest_math", ctypes.c_int, [ctypes.POINTER(_u64), ctypes.POINTER(_u
 _sig("ope_calibrate_surfaces", ctypes.c_int,
      [_i32, _vp, _vp, _vp, _sz, _vp, _sz, _vp, _vp, ctypes.POINTER(Options)])
 _sig("ope_calib_jacobian", ctypes.c_int, [_i32, _vp, _vp, _sz, _vp, _sz, _vp, _vp, _vp, ctypes.POINTER(Options)])
+_sig("ope_batch_implied_vol", ctypes.c_int, [_vp, _sz, _vp, _vp, _vp, ctypes.POINTER(Options)])
+_sig("ope_server_create", ctypes.c_int, [_vp, _vp])
+_sig("ope_server_destroy", ctypes.c_int, [_vp])
+_sig("ope_server_submit_price", ctypes.c_int, [_vp, _i32, _vp, _sz, _vp, ctypes.POINTER(_u64)])
+_sig("ope_server_submit_calibrate", ctypes.c_int, [_vp, _i32, _vp, _vp, _sz, _vp, ctypes.POINTER(_u64)])
+_sig("ope_server_wait", ctypes.c_int, [_vp, _u64, _d, _vp, _vp, ctypes.POINTER(_d)])
+_sig("ope_server_cancel", ctypes.c_int, [_vp, _u64])
+_sig("ope_server_get_stats", ctypes.c_int, [_vp, _vp])
 _sig("ope_measure_fp64_peak", ctypes.c_int, [ctypes.POINTER(_d), ctypes.POINTER(_d)])
 
 _lib = None

@@ -282,6 +282,18 @@ def calib_jacobian(model: int, quotes, iv_market, surf_offsets, params, tol=REF_
     return jac, res
 
 
+def batch_implied_vol(contracts, market_prices):
+    """batch.rs:51-56 on the device: (iv, ok); ok[i] is False where the reference returns None."""
+    con = contracts_array(contracts)
+    px = np.ascontiguousarray(market_prices, dtype=np.float64)
+    iv = np.zeros(con.size)
+    ok = np.zeros(con.size, np.int32)
+    if con.size:
+        check(load().ope_batch_implied_vol(con.ctypes.data, con.size, px.ctypes.data, iv.ctypes.data, ok.ctypes.data,
+                                           None))
+    return iv, ok.astype(bool)
+
+
 def measure_fp64_peak() -> tuple[float, float]:
     """(flop/s, ms) of the DFMA throughput probe on the current device."""
     f, ms = ctypes.c_double(), ctypes.c_double()
@@ -328,5 +340,5 @@ __all__ = [
     "heston_price", "bates_price", "batch_heston", "batch_bates", "batch_heston_greeks", "batch_bates_greeks",
     "price_surfaces", "price_surfaces_device", "batch_price_device", "contracts_array", "REF_TOL",
     "MODEL_HESTON", "MODEL_BATES", "RESULT_DTYPE", "kernel_launch_count", "device_info", "measure_fp64_peak", "price_gradient_surfaces",
-    "CALIB_RESULT_DTYPE", "calibrate_surfaces", "calibrate_heston", "calibrate_bates", "calib_jacobian",
+    "CALIB_RESULT_DTYPE", "batch_implied_vol", "calibrate_surfaces", "calibrate_heston", "calibrate_bates", "calib_jacobian",
 ]
