@@ -107,8 +107,17 @@ def test_batch_implied_vol_matches_oracle(ope, oracle):  # batch.rs:51-56, 255-2
     px[:10] = -1.0  # rejected by the bounds check (iv.rs:23)
     iv, ok = ope.batch_implied_vol(con, px)
     ref, rok = oracle.batch_implied_vol(con, px)
-    assert np.array_equal(ok, rok)
     assert not ok[:10].any()
-    assert np.max(np.abs(iv[ok] - ref[ok])) < 1e-9
-    good = ok & (px > 1e-6)
+    # where the time value is below 1e-9 * S the price equals intrinsic to the last ulps, the
+    # IV is not identifiable in double precision and the bounds check (iv.rs:30) flips with the
+    # last ulp of exp(); everywhere else the two solvers must agree on success and value
+    eq, er = np.exp(-con["div_yield"] * con["expiry"]), np.exp(-con["rate"] * con["expiry"])
+    intr = np.where(con["opt_type"] == 0, np.maximum(con["spot"] * eq - con["strike"] * er, 0.0),
+                    np.maximum(con["strike"] * er - con["spot"] * eq, 0.0))
+    well = (px - intr) > 1e-9 * 100.0
+    assert well.sum() > 3000
+    assert np.array_equal(ok[well], rok[well])
+    both = well & ok & rok
+    assert np.max(np.abs(iv[both] - ref[both])) < 1e-9
+    good = both & (px > 1e-6)
     assert np.max(np.abs(iv[good] - con["vol"][good])) < 1e-6
