@@ -246,6 +246,23 @@ int ope_price_surfaces_stats(int32_t model, const ope_contract* contracts, size_
  * device.  The roofline denominator for the FP64-bound pricing kernels. */
 int ope_measure_fp64_peak(double* flops_per_s, double* elapsed_ms);
 
+/* No counterpart in the reference.  For callers that cannot let a library
+ * allocate device memory -- pricing under stream capture (where cudaMalloc is
+ * not allowed), latency paths that cannot take cudaMalloc/cudaFree's device
+ * synchronisation, hosts whose device memory belongs to another allocator --
+ * this is ope_price_surfaces with DEVICE pointers only that allocates nothing:
+ * the kernel's scratch lives in a static device array of this library (about
+ * 1.25 MiB on every GPU that loads it, held until exit), so n is limited to
+ * OPE_NOALLOC_MAX_CONTRACTS (larger n: OPE_ERR_INVALID_ARG).  Stream-ordered
+ * on `stream` (cudaStream_t, NULL = legacy default stream).  The first call on
+ * a device looks up the array's device address; make it before any stream
+ * capture.  Every call shares the one array, so calls whose work overlaps on
+ * the GPU race: serialise them on one stream (or order them with events). */
+#define OPE_NOALLOC_MAX_CONTRACTS 65536
+int ope_price_surfaces_noalloc(int32_t model, const ope_contract* d_contracts, size_t n,
+                               const int64_t* d_surf_offsets, size_t n_surf, const void* d_params,
+                               double* d_out_prices, double tol, void* stream);
+
 /* No reference twin (numerics self-check): the worst error, in ulps, of the
  * kernels' Newton-refined reciprocal and square root against IEEE 1/x and
  * sqrt over 2^20 inputs spanning 1e-300 .. 1e300. */
