@@ -56,6 +56,9 @@ def parse_args():
     ap.add_argument("--plain-surfaces", type=int, default=256)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-calib", action="store_true", help="skip the config-4 calibration section")
+    ap.add_argument("--no-serving", action="store_true", help="skip the config-5 serving section")
+    ap.add_argument("--serving-rates", default="100,1000,5000,20000")
     return ap.parse_args()
 
 
@@ -178,6 +181,71 @@ class ClockSampler:
                         reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
                 "samples_under_load": len(sm)}
+
+
+def bench_calibration(args) -> dict:
+    """Config 4: 256 Heston surfaces x 300 quotes, LM in IV space on the device
+    (one conditional-WHILE graph), against the reference's LM (the oracle:
+    finite-difference Jacobian, calibration.rs:433-569) on the host cores."""
+    import ope_b200 as ope
+    from ope_b200 import workloads as W
+
+    def price_fn(con, params, sidx):
+        off = np.concatenate([[0], np.cumsum(np.bincount(sidx, minlength=params.shape[0]))])
+        return ope.price_surfaces(ope.MODEL_HESTON, con, off, params, tol=1e-10)
+
+    con, iv, off, true_p, p0 = W.c4(price_fn, ope.batch_implied_vol)
+    ope.calibrate_surfaces(ope.MODEL_HESTON, con, iv, off, p0)  # builds the graph
+    ts = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        r = ope.calibrate_surfaces(ope.MODEL_HESTON, con, iv, off, p0)
+        ts.append(time.perf_counter() - t0)
+    n_surf = off.size - 1
+    out = {
+        "workload": "c4-heston-256-surfaces-30x10-noise0.005", "quotes": int(con.size), "surfaces": int(n_surf),
+        "value": n_surf / min(ts), "unit": "surfaces/s", "ms": 1e3 * min(ts),
+        "iters_mean": float(r["iters"].mean()), "iters_max": int(r["iters"].max()),
+        "stopped_converged": int((r["status"] == 1).sum()), "stopped_damping_cap": int((r["status"] == 2).sum()),
+        "stopped_iteration_cap": int((r["status"] == 3).sum()), "rmse_median": float(np.median(r["rmse"])),
+        "jacobian": "adjoint kernel / BSM vega (exact)", "loop": "one CUDA graph launch (conditional WHILE node)",
+    }
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+
+        O.build()
+        k = max(2, min(O.max_threads(), 8))
+        t0 = time.perf_counter()
+        ro = O.calibrate_many(5, con[:off[k]], iv[:off[k]], off[:k + 1], p0[:k])
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": k / dt, "unit": "surfaces/s", "cores": min(k, O.max_threads()),
+                               "kind": "port", "sample": f"{k} surfaces, reference LM with FD Jacobian, "
+                                                         f"one surface per thread, {dt:.1f} s",
+                               "rmse_max_abs_diff_vs_gpu": float(np.max(np.abs(ro["rmse"] - r["rmse"][:k])))}
+    return out
+
+
+def bench_serving(args) -> dict:
+    """Config 5: Poisson arrivals, 80 % Bates surface reprices / 20 % Heston
+    calibrations, sizes log-uniform in [20, 2000] contracts, rates swept."""
+    from ope_b200 import serving as SV
+
+    out = {"mix": "80% Bates reprice / 20% Heston calibration, sizes log-uniform [20, 2000]", "rates": []}
+    pool = SV.make_stream(1200, seed=5)
+    with SV.Server(hbm_fraction=0.25, max_inflight=4) as srv:
+        # warm: one request of each kind
+        for r in pool[:8]:
+            rid = srv.submit_price(1, r.contracts, r.params) if r.kind == 0 else srv.submit_calibrate(
+                0, r.contracts, r.iv, r.params)
+            srv.wait(rid)
+        for rate in [float(x) for x in args.serving_rates.split(",")]:
+            n = int(min(len(pool), max(150, rate * 1.5)))
+            res = SV.run_stream(srv, pool[:n], rate, seed=int(rate))
+            out["rates"].append(SV.summarize(res))
+        st = srv.stats()
+    out["server"] = {k: st[k] for k in ("batches", "batched_requests", "max_inflight", "rejected",
+                                         "hbm_budget_bytes", "hbm_peak_bytes")}
+    return out
 
 
 def read_traffic():
@@ -343,6 +411,10 @@ def run_ours(args) -> None:
         rate, m, dt, cores = cpu_sample(w, args.cpu_seconds)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
                                 "sample": f"{m} random contracts of the workload in {dt:.1f} s"}
+    if rank == 0 and world == 1 and not args.no_calib:
+        line["calibration"] = bench_calibration(args)
+    if rank == 0 and world == 1 and not args.no_serving:
+        line["serving"] = bench_serving(args)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:
