@@ -64,8 +64,9 @@ def parse_args():
 
 def workload(n: int, rank: int):
     from ope_b200 import workloads as W
+    from ope_b200.multi import shard_seed
 
-    return W.c3(n=n, per_surface=256, seed=3 + rank)
+    return W.c3(n=n, per_surface=256, seed=shard_seed(3, rank))
 
 
 def config_of(w, world: int) -> dict:
@@ -108,7 +109,7 @@ def run_reference(args) -> None:
     if rank != 0:
         return
     w = workload(args.n, 0)
-    per_step = max(1.0, min(8.0, 60.0 / max(1, args.steps + args.warmup)))
+    per_step = max(0.2, min(args.cpu_seconds, 60.0 / max(1, args.steps + args.warmup)))
     for _ in range(args.warmup):
         cpu_sample(w, per_step / 4, rng_seed=17)
     rates, total_m, total_t, cores = [], 0, 0.0, 1
@@ -264,28 +265,17 @@ def run_ours(args) -> None:
     import ope_b200 as ope
     from ope_b200 import roofline
 
-    rank = int(os.environ.get("RANK", "0"))
-    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
+    from ope_b200 import multi
+
+    rank, local_rank, world = multi.rank_info()
     torch.cuda.set_device(local_rank)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dist = multi.init("nccl")
 
     def barrier():
-        if dist is not None:
-            dist.barrier()
+        multi.barrier(dist)
 
     def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return multi.max_over_ranks(dist, x, device="cuda")
 
     w = workload(args.n, rank)
     n, n_surf = w.n, w.n_surf
@@ -337,7 +327,7 @@ def run_ours(args) -> None:
     region_ms = max_over_ranks(t_all0.elapsed_time(t_all1))
     kern_ms = [a.elapsed_time(b) for a, b in ev]
     kern_avg = statistics.mean(kern_ms)
-    value = world * n * args.steps / (region_ms * 1e-3)
+    value = multi.weak_scaling_value(world, n, args.steps, region_ms * 1e-3)
 
     # check this run's prices against the stats run (same bits expected)
     ref_prices = np.empty(n)
@@ -364,7 +354,7 @@ def run_ours(args) -> None:
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     clk = clocks.stop()  # sampled over both timed regions (device and e2e)
     barrier()
-    e2e_value = world * n * args.steps / e2e_s
+    e2e_value = multi.weak_scaling_value(world, n, args.steps, e2e_s)
     h2d = n * 56 + (n_surf + 1) * 8 + n_surf * 8 * 8
     d2h = n * 8
 

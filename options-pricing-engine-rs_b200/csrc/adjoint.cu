@@ -22,6 +22,12 @@
 #include "internal.h"
 #include "quadrature.cuh"
 
+// Minimum resident blocks per SM for the adjoint kernel's __launch_bounds__
+// (caps registers per thread at 65536 / (128 * OPE_GRAD_MINB)).
+#ifndef OPE_GRAD_MINB
+#define OPE_GRAD_MINB 1
+#endif
+
 namespace ope {
 
 namespace {
@@ -42,7 +48,7 @@ __device__ __forceinline__ long long find_surface_g(const int64_t* off, long lon
 }
 
 template <bool BATES>
-__global__ void __launch_bounds__(128) k_price_grad(const ope_contract* __restrict__ con, long long n,
+__global__ void __launch_bounds__(128, OPE_GRAD_MINB) k_price_grad(const ope_contract* __restrict__ con, long long n,
                                                     const int64_t* __restrict__ surf_off, long long n_surf,
                                                     const int32_t* __restrict__ param_idx,
                                                     const int32_t* __restrict__ surf_mask,
