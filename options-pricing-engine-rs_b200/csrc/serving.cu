@@ -160,10 +160,24 @@ size_t price_job_dev_bytes(size_t n, size_t ns, int dim) {
 // Returns true if something was launched.
 bool launch_batch(Server& S, int slot) {
     if (S.pending.empty()) return false;
-    // the oldest pending request decides kind and model; take every pending
-    // request of that kind/model, FIFO, while the batch still fits the
-    // contract limit and the admission budget (the whole slab)
-    const int kind = S.pending.front()->kind, model = S.pending.front()->model;
+    // Reprices go first: they are short, and a calibration batch runs a whole
+    // LM loop.  The oldest pending reprice decides the model; without pending
+    // reprices the oldest calibration does, but calibration batches never take
+    // the last free slot, so an arriving reprice always finds a stream.  Every
+    // pending request of the chosen kind/model is taken, FIFO, while the batch
+    // still fits the contract limit and the admission budget (the whole slab).
+    const Request* first_price = nullptr;
+    const Request* first_calib = nullptr;
+    for (const auto& r : S.pending) {
+        if (r->kind == RK_PRICE && !first_price) first_price = r.get();
+        if (r->kind == RK_CALIB && !first_calib) first_calib = r.get();
+    }
+    size_t calib_inflight = 0;
+    for (const auto& j : S.inflight) calib_inflight += j.kind == RK_CALIB;
+    const Request* lead = first_price;
+    if (!lead && first_calib && (calib_inflight + 1 < S.streams.size() || S.streams.size() == 1)) lead = first_calib;
+    if (!lead) return false;
+    const int kind = lead->kind, model = lead->model;
     const int dim = param_stride(model);
     auto dev_need = [&](size_t n, size_t ns) {
         return kind == RK_PRICE ? price_job_dev_bytes(n, ns, dim) : calib_workspace_bytes(n, ns, dim);
