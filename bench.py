@@ -84,8 +84,11 @@ def config_of(w, world: int) -> dict:
 
 
 # ----------------------------------------------------------------- CPU side
-def cpu_sample(w, seconds: float, rng_seed: int = 0):
-    """Time the oracle (all host cores) on a random contract sample sized to ~`seconds`."""
+def cpu_sample(w, seconds: float, rng_seed: int = 0, gpu_prices=None):
+    """Time the oracle (all host cores) on a random contract sample sized to ~`seconds`.
+
+    With gpu_prices (the GPU's prices for the whole workload) also returns the
+    worst |gpu - oracle| over the sample: the per-contract parity check."""
     from oracle import oracle as O
 
     O.build()
@@ -98,8 +101,11 @@ def cpu_sample(w, seconds: float, rng_seed: int = 0):
     m = int(min(w.n, max(2048, rate * seconds)))
     idx = np.sort(rng.choice(w.n, m, replace=False))
     t0 = time.perf_counter()
-    O.batch_price(w.contracts[idx], w.params, True, w.tol, surf_idx=si[idx])
+    ref = O.batch_price(w.contracts[idx], w.params, True, w.tol, surf_idx=si[idx])
     dt = time.perf_counter() - t0
+    if gpu_prices is not None:
+        err = np.abs(gpu_prices[idx] - ref) / w.contracts["spot"][idx]
+        return m / dt, m, dt, O.max_threads(), float(err.max())
     return m / dt, m, dt, O.max_threads()
 
 
@@ -366,9 +372,12 @@ def run_ours(args) -> None:
     barrier()
     t0 = time.perf_counter()
     cnt = 0
+    call_ms = []
     for s in picks:
         c = w.contracts[w.surf_offsets[s]:w.surf_offsets[s + 1]]
+        t1 = time.perf_counter()
         ope.batch_bates(c, w.params[s], tol=w.tol)
+        call_ms.append(1e3 * (time.perf_counter() - t1))
         cnt += c.size
     plain_s = max_over_ranks(time.perf_counter() - t0)
     plain_value = world * cnt / plain_s
@@ -386,7 +395,9 @@ def run_ours(args) -> None:
                 "api": "ope_price_surfaces (host pointers, pinned)"},
         "plain": {"value": plain_value, "unit": UNIT, "surfaces_sampled": int(picks.size),
                   "api": "ope_batch_bates per surface (host pointers, synchronous)",
-                  "batched_e2e_over_plain": e2e_value / plain_value},
+                  "batched_e2e_over_plain": e2e_value / plain_value,
+                  "latency_ms_per_256_contract_surface": {"p50": float(np.percentile(call_ms, 50)),
+                                                          "p99": float(np.percentile(call_ms, 99))}},
         "roofline": {"bound": "fp64", "achieved": achieved / 1e12, "peak": peak_flops / 1e12, "unit": "TFLOP/s",
                      "frac": achieved / peak_flops, "traffic": traffic,
                      "peak_source": "measured DFMA-chain probe on this GPU (ope_measure_fp64_peak)",
@@ -398,9 +409,11 @@ def run_ours(args) -> None:
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, m, dt, cores = cpu_sample(w, args.cpu_seconds)
+        rate, m, dt, cores, worst = cpu_sample(w, args.cpu_seconds, gpu_prices=ref_prices)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
                                 "sample": f"{m} random contracts of the workload in {dt:.1f} s"}
+        line["parity"] = {"max_abs_err_over_spot": worst, "bar": 1e-9, "contracts_checked": m,
+                          "against": "CPU oracle (the reference restated), same tolerance, same contracts"}
     if rank == 0 and world == 1 and not args.no_calib:
         line["calibration"] = bench_calibration(args)
     if rank == 0 and world == 1 and not args.no_serving:
