@@ -25,7 +25,7 @@
 // Minimum resident blocks per SM for the adjoint kernel's __launch_bounds__
 // (caps registers per thread at 65536 / (128 * OPE_GRAD_MINB)).
 #ifndef OPE_GRAD_MINB
-#define OPE_GRAD_MINB 1
+#define OPE_GRAD_MINB 5
 #endif
 
 namespace ope {
@@ -71,7 +71,13 @@ __global__ void __launch_bounds__(128, OPE_GRAD_MINB) k_price_grad(const ope_con
         const int which = (int)(unit & 1);
         const long long s = param_idx ? (long long)__ldg(param_idx + c)
                                       : (n_surf > 1 ? find_surface_g(surf_off, n_surf, c) : 0);
-        if (surf_mask && __ldg(surf_mask + s) == 0) continue;
+        if (surf_mask && __ldg(surf_mask + s) == 0) {
+            // a skipped surface's units are contiguous: move the queue head past
+            // all of them with one atomic instead of one per unit
+            if (lane == 0 && !param_idx && surf_off)
+                atomicMax(head, 2ull * (unsigned long long)__ldg(surf_off + s + 1));
+            continue;
+        }
         const double* p = params + s * DIM;
         double pl[8];
 #pragma unroll

@@ -124,7 +124,13 @@ __global__ void __launch_bounds__(OPE_KERNEL_WARPS * 32, OPE_KERNEL_MINB) k_pric
         const long long c = (long long)(unit >> 1);
         const long long s = param_idx ? (long long)__ldg(param_idx + c)
                                       : (n_surf > 1 ? find_surface(surf_off, n_surf, c) : 0);
-        if (surf_mask && __ldg(surf_mask + s) == 0) continue;
+        if (surf_mask && __ldg(surf_mask + s) == 0) {
+            // a skipped surface's units are contiguous: move the queue head past
+            // all of them with one atomic instead of one per unit
+            if (lane == 0 && !param_idx && surf_off)
+                atomicMax(head, 2ull * (unsigned long long)__ldg(surf_off + s + 1));
+            continue;
+        }
         run_unit<BATES>(c, (int)(unit & 1), con, params + s * stride, tol, out, integ, done, nbis_out,
                         smem_panels[warp], lane, R);
     }
