@@ -196,7 +196,10 @@ int ope_price_gradient_surfaces(int32_t model, const ope_contract* contracts, si
  * are still running and their work overlaps on the GPU.  Admission is by
  * device memory: the server reserves hbm_fraction of the FREE HBM at creation
  * (capped by hbm_cap_bytes) and launches a batch when its buffers fit; a
- * request that can never fit is rejected (OPE_ERR_REJECTED).  A request's
+ * request that can never fit is rejected (OPE_ERR_REJECTED).  Reprices run
+ * on high-priority streams; calibrations one batch at a time on a
+ * low-priority stream, its kernels' grids capped at calib_sm_fraction of the
+ * block slots, so a reprice's blocks find free slots while a calibration runs.  A request's
  * results do not depend on what it was batched with. */
 typedef struct ope_server ope_server;
 
@@ -207,6 +210,8 @@ typedef struct {
     uint32_t max_inflight;         /* concurrent micro-batches = streams (0 -> 4) */
     uint32_t max_batch_contracts;  /* contracts per micro-batch (0 -> 2^20) */
     uint64_t pinned_bytes;         /* host staging (0 -> 256 MiB) */
+    double calib_sm_fraction;      /* share of the GPU's block slots a calibration batch's kernels may fill,
+                                      leaving the rest to reprices (<= 0 or > 1 -> 0.5) */
 } ope_server_config;
 
 typedef struct {

@@ -153,7 +153,8 @@ int grad_grid(K kernel, size_t smem, unsigned long long need, int* grid) {
     OPE_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     OPE_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 128, smem));
     if (per_sm < 1) per_sm = 1;
-    *grid = (int)std::min<unsigned long long>((unsigned long long)per_sm * tctx().sm_count, need);
+    const int cap = std::max(1, (int)(per_sm * tctx().sm_count * tctx().grid_fraction));
+    *grid = (int)std::min<unsigned long long>((unsigned long long)cap, need);
     return OPE_OK;
 }
 

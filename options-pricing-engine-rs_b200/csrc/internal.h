@@ -26,6 +26,7 @@ struct ThreadCtx {
     size_t pinned_bytes = 0;
     std::string last_error;
     uint64_t launches = 0;
+    double grid_fraction = 1.0;  // persistent launches fill at most this share of the block slots
 };
 
 ThreadCtx& tctx();

@@ -142,7 +142,7 @@ int persistent_grid(K kernel, int threads, size_t smem, int* grid) {
     OPE_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     OPE_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem));
     if (per_sm < 1) per_sm = 1;
-    *grid = per_sm * tctx().sm_count;
+    *grid = std::max(1, (int)(per_sm * tctx().sm_count * tctx().grid_fraction));
     return OPE_OK;
 }
 

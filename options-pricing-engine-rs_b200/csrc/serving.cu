@@ -6,12 +6,19 @@
 // the GPU through the same kernels:
 //
 //  * submit() copies a request into host memory and queues it (non-blocking);
-//  * one scheduler thread forms micro-batches from everything pending
-//    whenever an in-flight slot (a CUDA stream) and device memory are free:
-//    all pending reprices of one model go into ONE multi-surface persistent
-//    launch (each request is a surface with its own parameters), pending
-//    calibrations into ONE batched device-LM run (one conditional-WHILE
-//    graph);
+//  * two scheduler threads, one per request kind, form micro-batches from
+//    everything pending whenever an in-flight slot and device memory are
+//    free: all pending reprices of one model go into ONE multi-surface
+//    persistent launch (each request is a surface with its own parameters),
+//    pending calibrations into ONE batched device-LM run (one
+//    conditional-WHILE graph).  The slow host part of a calibration batch
+//    (graph capture and instantiation) runs on its own thread outside the
+//    server lock, so it never delays a reprice launch;
+//  * reprices run on high-priority streams; calibrations run one batch at a
+//    time on low-priority streams with their kernels' grids capped at a share
+//    of the GPU's block slots: a reprice's blocks are scheduled ahead of
+//    queued calibration blocks and find free slots on every SM while a
+//    calibration runs;
 //  * admission is by device memory: at creation the server reserves a slab
 //    of a configurable fraction of the FREE HBM (cudaMemGetInfo); a batch is
 //    launched when its buffers fit in the slab, requests that can never fit
@@ -135,7 +142,7 @@ struct Server {
     void* dev_base = nullptr;
     char* pin_base = nullptr;
     std::unique_ptr<Slab> dev_slab, pin_slab;
-    std::vector<cudaStream_t> streams;
+    std::vector<cudaStream_t> streams_hi, streams_lo;  // per slot: reprice / calibration streams
     std::vector<bool> slot_busy;
     std::mutex mu;
     std::condition_variable cv_sched, cv_done;
@@ -143,7 +150,7 @@ struct Server {
     std::map<uint64_t, std::shared_ptr<Request>> all;
     std::vector<Job> inflight;
     std::atomic<bool> stop{false};
-    std::thread thr;
+    std::thread thr_price, thr_calib;
     uint64_t next_id = 1;
     ope_server_stats stats{};
     std::string fatal;
@@ -156,28 +163,34 @@ size_t price_job_dev_bytes(size_t n, size_t ns, int dim) {
            align_up(ns * dim * sizeof(double), 256) + align_up(n * sizeof(double), 256) + price_scratch_bytes(n);
 }
 
-// Form and launch one micro-batch from the pending queue (caller holds mu).
-// Returns true if something was launched.
-bool launch_batch(Server& S, int slot) {
+// Form and launch one micro-batch of `kind` from the pending queue.  Called
+// with `lk` held; the lock is released while the batch is packed and
+// enqueued, and held again on return.  Returns true if something was launched.
+bool launch_batch(Server& S, int kind, std::unique_lock<std::mutex>& lk) {
     if (S.pending.empty()) return false;
-    // Reprices go first: they are short, and a calibration batch runs a whole
-    // LM loop.  The oldest pending reprice decides the model; without pending
-    // reprices the oldest calibration does, but calibration batches never take
-    // the last free slot, so an arriving reprice always finds a stream.  Every
-    // pending request of the chosen kind/model is taken, FIFO, while the batch
-    // still fits the contract limit and the admission budget (the whole slab).
-    const Request* first_price = nullptr;
-    const Request* first_calib = nullptr;
-    for (const auto& r : S.pending) {
-        if (r->kind == RK_PRICE && !first_price) first_price = r.get();
-        if (r->kind == RK_CALIB && !first_calib) first_calib = r.get();
+    // A free slot; calibration batches never take the last free one, so an
+    // arriving reprice always finds a slot.
+    int slot = -1;
+    size_t n_free = 0;
+    for (size_t i = 0; i < S.slot_busy.size(); ++i)
+        if (!S.slot_busy[i]) { n_free += 1; if (slot < 0) slot = (int)i; }
+    if (slot < 0) return false;
+    if (kind == RK_CALIB) {
+        // one calibration batch at a time (later ones join the next batch), and
+        // never in the last free slot: with its grids capped, the rest of the
+        // GPU's block slots and at least one stream stay free for reprices
+        if (n_free < 2 && S.slot_busy.size() > 1) return false;
+        for (const auto& j : S.inflight)
+            if (j.kind == RK_CALIB) return false;
     }
-    size_t calib_inflight = 0;
-    for (const auto& j : S.inflight) calib_inflight += j.kind == RK_CALIB;
-    const Request* lead = first_price;
-    if (!lead && first_calib && (calib_inflight + 1 < S.streams.size() || S.streams.size() == 1)) lead = first_calib;
+    // The oldest pending request of this kind decides the model; every pending
+    // request of that kind and model is taken, FIFO, while the batch still fits
+    // the contract limit and the admission budget (the whole slab).
+    const Request* lead = nullptr;
+    for (const auto& r : S.pending)
+        if (r->kind == kind) { lead = r.get(); break; }
     if (!lead) return false;
-    const int kind = lead->kind, model = lead->model;
+    const int model = lead->model;
     const int dim = param_stride(model);
     auto dev_need = [&](size_t n, size_t ns) {
         return kind == RK_PRICE ? price_job_dev_bytes(n, ns, dim) : calib_workspace_bytes(n, ns, dim);
@@ -225,6 +238,8 @@ bool launch_batch(Server& S, int slot) {
         requeue();
         return false;
     }
+    S.slot_busy[slot] = true;
+    for (auto& r : take) r->state = RQ_RUNNING;
     Job J;
     J.kind = kind;
     J.model = model;
@@ -234,10 +249,15 @@ bool launch_batch(Server& S, int slot) {
     J.dev_bytes = dev_bytes;
     J.pin_off = pin_off;
     J.pin_bytes = pin_bytes;
-    cudaStream_t st = S.streams[slot];
+    cudaStream_t st = kind == RK_PRICE ? S.streams_hi[slot] : S.streams_lo[slot];
     char* dev = static_cast<char*>(S.dev_base) + dev_off;
     char* pin = S.pin_base + pin_off;
-    // pack the batch in pinned memory: contracts, offsets, params
+    const double tol = S.tol;
+    const double calib_fraction = S.cfg.calib_sm_fraction;
+
+    // The requests, slot, device and pinned regions now belong to this batch:
+    // pack and enqueue without the lock.
+    lk.unlock();
     char* p = pin;
     ope_contract* con_h = reinterpret_cast<ope_contract*>(p);
     p += align_up(n * sizeof(ope_contract), 256);
@@ -253,7 +273,6 @@ bool launch_batch(Server& S, int slot) {
         std::memcpy(par_h + s * dim, r.params.data(), dim * sizeof(double));
         at += r.con.size();
         off_h[s + 1] = (int64_t)at;
-        r.state = RQ_RUNNING;
     }
     int rc = OPE_OK;
     if (kind == RK_PRICE) {
@@ -273,7 +292,7 @@ bool launch_batch(Server& S, int slot) {
         if (rc == OPE_OK)
             rc = check_cuda(cudaMemcpyAsync(d_par, par_h, ns * dim * sizeof(double), cudaMemcpyHostToDevice, st), "h2d");
         if (rc == OPE_OK)
-            rc = launch_price_persistent(model, d_con, n, d_off, ns, nullptr, d_par, S.tol, d_out,
+            rc = launch_price_persistent(model, d_con, n, d_off, ns, nullptr, d_par, tol, d_out,
                                          carve_price_scratch(d, n), st);
         if (rc == OPE_OK)
             rc = check_cuda(cudaMemcpyAsync(J.prices_h, d_out, n * sizeof(double), cudaMemcpyDeviceToHost, st), "d2h");
@@ -289,29 +308,38 @@ bool launch_batch(Server& S, int slot) {
         p += align_up(calib_pinned_bytes(n, ns, dim), 256);
         J.calib_h = reinterpret_cast<ope_calib_result*>(p);
         J.graph = calib_graph_new();
-        rc = calib_enqueue(model, con_h, iv_h, nullptr, n, off_h, off_h, ns, par_h, J.calib_h, S.tol,
+        // this thread's persistent launches (captured into the LM graph) leave
+        // the rest of the block slots to reprices
+        ThreadCtx& c = tctx();
+        c.grid_fraction = calib_fraction;
+        rc = calib_enqueue(model, con_h, iv_h, nullptr, n, off_h, off_h, ns, par_h, J.calib_h, tol,
                            cudaMemcpyHostToDevice, cudaMemcpyDeviceToHost, dev, cpin, st, J.graph);
+        c.grid_fraction = 1.0;
     }
     if (rc == OPE_OK) rc = check_cuda(cudaEventCreateWithFlags(&J.done, cudaEventDisableTiming), "event");
     if (rc == OPE_OK) rc = check_cuda(cudaEventRecord(J.done, st), "event");
+    const std::string err = rc != OPE_OK ? tctx().last_error : std::string();
     if (rc != OPE_OK) {
         cudaStreamSynchronize(st);
         cudaGetLastError();
+        if (J.done) cudaEventDestroy(J.done);
+        if (J.graph) calib_graph_delete(J.graph);
+    }
+    lk.lock();
+    if (rc != OPE_OK) {
         for (auto& r : take) {
             r->state = RQ_FAILED;
             r->error = rc;
-            r->message = tctx().last_error;
+            r->message = err;
             r->t_done = Clock::now();
         }
-        if (J.done) cudaEventDestroy(J.done);
-        if (J.graph) calib_graph_delete(J.graph);
         S.dev_slab->release(dev_off, dev_bytes);
         S.pin_slab->release(pin_off, pin_bytes);
+        S.slot_busy[slot] = false;
         S.stats.failed += ns;
         S.cv_done.notify_all();
         return false;
     }
-    S.slot_busy[slot] = true;
     S.stats.batches += 1;
     S.stats.batched_requests += ns;
     S.inflight.push_back(J);
@@ -360,34 +388,21 @@ bool retire(Server& S) {
     return any;
 }
 
-void scheduler(Server* S) {
+// One scheduler thread per request kind: retire finished batches, launch
+// batches of its kind while slots and memory allow, sleep briefly.
+void scheduler(Server* S, int kind) {
     cudaSetDevice(S->device);
     ensure_device();
     std::unique_lock<std::mutex> lk(S->mu);
     while (!S->stop.load()) {
         retire(*S);
-        bool launched = true;
-        while (launched && !S->pending.empty()) {
-            launched = false;
-            for (size_t s = 0; s < S->streams.size(); ++s) {
-                if (!S->slot_busy[s]) {
-                    launched = launch_batch(*S, (int)s);
-                    break;
-                }
-            }
+        while (!S->stop.load() && launch_batch(*S, kind, lk)) {
         }
         // sleep until a submit arrives, or briefly while work is in flight
         if (S->inflight.empty() && S->pending.empty())
             S->cv_sched.wait_for(lk, std::chrono::milliseconds(5));
         else
             S->cv_sched.wait_for(lk, std::chrono::microseconds(20));
-    }
-    // drain
-    while (!S->inflight.empty()) {
-        lk.unlock();
-        std::this_thread::sleep_for(std::chrono::microseconds(50));
-        lk.lock();
-        retire(*S);
     }
 }
 
@@ -412,7 +427,7 @@ int submit(Server* S, int kind, int model, const ope_contract* con, size_t n, co
         S->pending.push_back(r);
         S->stats.submitted += 1;
     }
-    S->cv_sched.notify_one();
+    S->cv_sched.notify_all();
     *out_id = r->id;
     return OPE_OK;
 }
@@ -435,6 +450,7 @@ int ope_server_create(const ope_server_config* cfg, ope_server** out) {
     if (S->cfg.max_inflight == 0) S->cfg.max_inflight = 4;
     if (S->cfg.max_batch_contracts == 0) S->cfg.max_batch_contracts = 1u << 20;
     if (S->cfg.pinned_bytes == 0) S->cfg.pinned_bytes = 256ull << 20;
+    if (!(S->cfg.calib_sm_fraction > 0.0 && S->cfg.calib_sm_fraction <= 1.0)) S->cfg.calib_sm_fraction = 0.5;
     S->tol = S->cfg.tol > 0.0 ? S->cfg.tol : OPE_REF_TOL;
     cudaGetDevice(&S->device);
     size_t free_b = 0, total_b = 0;
@@ -451,11 +467,16 @@ int ope_server_create(const ope_server_config* cfg, ope_server** out) {
     S->pin_base = static_cast<char*>(pin);
     S->dev_slab.reset(new Slab(budget));
     S->pin_slab.reset(new Slab(S->cfg.pinned_bytes));
-    S->streams.resize(S->cfg.max_inflight);
+    S->streams_hi.resize(S->cfg.max_inflight);
+    S->streams_lo.resize(S->cfg.max_inflight);
     S->slot_busy.assign(S->cfg.max_inflight, false);
-    for (auto& st : S->streams) cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    int prio_lo = 0, prio_hi = 0;  // numerically lower = higher priority
+    cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+    for (auto& st : S->streams_hi) cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, prio_hi);
+    for (auto& st : S->streams_lo) cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, prio_lo);
     S->stats.hbm_budget_bytes = budget;
-    S->thr = std::thread(scheduler, S);
+    S->thr_price = std::thread(scheduler, S, (int)RK_PRICE);
+    S->thr_calib = std::thread(scheduler, S, (int)RK_CALIB);
     *out = reinterpret_cast<ope_server*>(S);
     return OPE_OK;
 }
@@ -465,8 +486,19 @@ int ope_server_destroy(ope_server* srv) {
     if (!S) return OPE_OK;
     S->stop.store(true);
     S->cv_sched.notify_all();
-    if (S->thr.joinable()) S->thr.join();
-    for (auto& st : S->streams) cudaStreamDestroy(st);
+    if (S->thr_price.joinable()) S->thr_price.join();
+    if (S->thr_calib.joinable()) S->thr_calib.join();
+    {  // drain what is still in flight
+        std::unique_lock<std::mutex> lk(S->mu);
+        while (!S->inflight.empty()) {
+            lk.unlock();
+            std::this_thread::sleep_for(std::chrono::microseconds(50));
+            lk.lock();
+            retire(*S);
+        }
+    }
+    for (auto& st : S->streams_hi) cudaStreamDestroy(st);
+    for (auto& st : S->streams_lo) cudaStreamDestroy(st);
     cudaFree(S->dev_base);
     cudaFreeHost(S->pin_base);
     delete S;

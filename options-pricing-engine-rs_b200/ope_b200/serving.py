@@ -29,6 +29,7 @@ class ServerConfig(ctypes.Structure):
         ("max_inflight", ctypes.c_uint32),
         ("max_batch_contracts", ctypes.c_uint32),
         ("pinned_bytes", ctypes.c_uint64),
+        ("calib_sm_fraction", ctypes.c_double),
     ]
 
 
@@ -42,10 +43,11 @@ class Server:
     """A running server.  submit_* return request ids; wait() returns (result, latency_ms)."""
 
     def __init__(self, tol: float = api.REF_TOL, hbm_fraction: float = 0.5, hbm_cap_bytes: int = 0,
-                 max_inflight: int = 4, max_batch_contracts: int = 0, pinned_bytes: int = 0):
+                 max_inflight: int = 4, max_batch_contracts: int = 0, pinned_bytes: int = 0,
+                 calib_sm_fraction: float = 0.5):
         cfg = ServerConfig(tol=tol, hbm_fraction=hbm_fraction, hbm_cap_bytes=hbm_cap_bytes,
                            max_inflight=max_inflight, max_batch_contracts=max_batch_contracts,
-                           pinned_bytes=pinned_bytes)
+                           pinned_bytes=pinned_bytes, calib_sm_fraction=calib_sm_fraction)
         h = ctypes.c_void_p()
         check(load().ope_server_create(ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h
