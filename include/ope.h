@@ -79,13 +79,27 @@ typedef struct {
 
 /* calibration.rs:44-68 CalibResult.  params holds (v0, kappa, theta, sigma,
  * rho[, lambda, mu_j, sigma_j]); status: 1 converged (gradient or step
- * test), 2 stopped on the damping cap, 3 stopped on the iteration cap. */
+ * test), 2 stopped on the damping cap, 3 stopped on the iteration cap,
+ * 4 pruned by multistart (early_stopped). */
 typedef struct {
     double params[8];
     double rmse, max_err, condition_number;
     double weakest_direction[8];
     int32_t iters, converged, early_stopped, status;
 } ope_calib_result;
+
+/* calibration.rs:70-76 MultistartResult (+ the index of the best restart). */
+typedef struct {
+    ope_calib_result best;
+    int32_t n_restarts, n_converged, n_pruned, best_restart;
+} ope_multistart_result;
+
+/* calibration.rs:296-300 GlobalCalibResult (+ the population size used). */
+typedef struct {
+    ope_calib_result best;  /* after the LM polish */
+    double de_best_sse;     /* SSE of the DE winner, before the polish */
+    int32_t de_generations, n_pop;
+} ope_global_result;
 
 typedef struct {
     double tol;        /* absolute GK15 tolerance; <= 0 selects OPE_REF_TOL */
@@ -168,6 +182,45 @@ int ope_calibrate_surfaces(int32_t model, const ope_contract* quotes, const doub
                            const double* weights, size_t n_quotes, const int64_t* surf_offsets,
                            size_t n_surf, const double* p0, ope_calib_result* out,
                            const ope_options* opts);
+
+/* calibration.rs:220-230 calibrate_heston_regularized /
+ * calibrate_bates_regularized, batched like ope_calibrate_surfaces: surface s
+ * is pulled toward prior[s * dim ...] with weight reg_weight[s] (Tikhonov
+ * pseudo-rows (p_k - prior_k) / scale_k, scale = calibration.rs:130, 174-177);
+ * rmse, max_err and the J'J diagnostics stay data-only, as in the reference.
+ * prior and reg_weight are host pointers. */
+int ope_calibrate_surfaces_reg(int32_t model, const ope_contract* quotes, const double* iv_market,
+                               const double* weights, size_t n_quotes, const int64_t* surf_offsets, size_t n_surf,
+                               const double* p0, const double* prior, const double* reg_weight,
+                               ope_calib_result* out, const ope_options* opts);
+
+/* calibration.rs:246-314 calibrate_heston_multistart /
+ * calibrate_bates_multistart, batched over surfaces (host pointers).  Every
+ * surface runs n_restarts LM fits: restart 0 from p0[s], restart i from
+ * CalibModel::random_guess (calibration.rs:131-141, 179-185) under rand 0.8's
+ * SmallRng::seed_from_u64(splitmix64(seed ^ i)) (every surface gets the same
+ * starts, as one reference call per surface would).  The restarts of a
+ * surface share a best SSE and prune as the reference does (every 10
+ * iterations, SSE > 8x the shared best); on the device they advance in
+ * lockstep, one LM iteration each per pass.  shared_best0: NULL (+inf, the
+ * reference) or n_surf initial values.  out: n_surf records; out_restarts:
+ * NULL or n_surf x n_restarts records. */
+int ope_calibrate_multistart(int32_t model, const ope_contract* quotes, const double* iv_market,
+                             const double* weights, size_t n_quotes, const int64_t* surf_offsets, size_t n_surf,
+                             const double* p0, int32_t n_restarts, uint64_t seed, const double* shared_best0,
+                             ope_multistart_result* out, ope_calib_result* out_restarts, const ope_options* opts);
+
+/* calibration.rs:316-427 calibrate_heston_global / calibrate_bates_global
+ * (prior == NULL) and calibrate_*_global_regularized (prior: n_surf x dim,
+ * reg_weight: n_surf), batched over surfaces (host pointers): differential
+ * evolution DE/rand/1/bin (F 0.6, CR 0.9) over the parameter box with
+ * max(n_pop, 4 dim) members for n_gen generations, every member's SSE a
+ * device pricing + IV pass and the generation loop one CUDA graph launch,
+ * then one device LM polish from each surface's winner. */
+int ope_calibrate_global(int32_t model, const ope_contract* quotes, const double* iv_market, const double* weights,
+                         size_t n_quotes, const int64_t* surf_offsets, size_t n_surf, int32_t n_pop, int32_t n_gen,
+                         uint64_t seed, const double* prior, const double* reg_weight, ope_global_result* out,
+                         const ope_options* opts);
 
 /* calibration.rs:613-652 jacobian (host pointers): the IV-space Jacobian the
  * device LM uses, d iv_i / d p = (d price_i / d p) / vega_BSM(iv_i), rows of

@@ -19,6 +19,18 @@
 // after an accepted step (the reference recomputes the same J after a
 // rejected or out-of-bounds step).
 //
+// Optional per surface (CalibExtra): a Tikhonov prior, added as dim pseudo
+// rows (p_k - prior_k) / scale_k of weight sqrt(reg_weight) to the SSE, J'J
+// and J'r exactly as calibration.rs:448-470 appends them (the final rmse,
+// max error and J'J diagnostics stay data-only, calibration.rs:541-568); and
+// a restart group for multistart pruning: members publish every accepted SSE
+// to the group's shared best (atomicMin on the bits of a non-negative
+// double) and, at iterations 10, 20, ..., stop (early_stopped) when their SSE
+// exceeds 8x that best (calibration.rs:263-264, 482-490).  All surfaces take
+// one LM iteration per pass, so every check in pass k sees exactly the
+// accepted steps of passes < k: the restarts run in lockstep, one of the
+// schedules the reference's thread-timed sharing allows.
+//
 // One LM iteration for ALL surfaces is one pass of the body below; the body
 // is captured once into a CUDA graph whose conditional WHILE node repeats it
 // on the device until every surface has stopped: one graph launch per
@@ -36,8 +48,10 @@ namespace ope {
 
 namespace {
 
-enum { LM_ACTIVE = 0, LM_CONVERGED = 1, LM_BAILED = 2, LM_MAXITER = 3 };
+enum { LM_ACTIVE = 0, LM_CONVERGED = 1, LM_BAILED = 2, LM_MAXITER = 3, LM_PRUNED = 4 };
 constexpr int kMaxIter = 200;
+constexpr int kPruneEvery = 10;          // calibration.rs:264
+constexpr double kPruneFactor = 8.0;     // calibration.rs:263
 constexpr double kTolGrad = 1e-8, kTolParams = 1e-10, kLamInit = 1e-3, kLamUp = 10.0, kLamDown = 0.1,
                  kLamMax = 1e8;
 
@@ -66,7 +80,30 @@ struct LMDev {
     double* res_new; // nq
     double* jrow;    // nq x dim
     unsigned int* counters;  // [0] active surfaces, [1] body passes
+    const double* prior;     // ns x dim Tikhonov prior, or null
+    const double* regw;      // ns regularisation weights
+    const int32_t* group;    // ns restart groups, or null (no pruning)
+    unsigned long long* gbest;  // per group: shared best SSE (bits of a non-negative double)
 };
+
+// calibration.rs:130, 174-177 regularization_scale
+__device__ __forceinline__ double reg_scale(int k) {
+    constexpr double s[8] = {0.04, 2.0, 0.04, 0.3, 0.3, 0.5, 0.1, 0.15};
+    return s[k];
+}
+
+// The Tikhonov rows' share of the weighted SSE, added after the data rows in
+// row order (calibration.rs:460-465, 589-591).
+__device__ double add_reg_sse(const LMDev& D, int s, const double* p, double sse) {
+    if (!D.prior) return sse;
+    const double rw = sqrt(D.regw[s]);
+    for (int k = 0; k < D.dim; ++k) {
+        const double r = (p[k] - D.prior[s * D.dim + k]) / reg_scale(k);
+        const double t = rw * r;
+        sse = sse + t * t;
+    }
+    return sse;
+}
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -256,14 +293,37 @@ __global__ void k_lm_step(LMDev D) {
     S.need_jac = 0;
     D.jmask[s] = 0;
     S.iters += 1;
+    const int iter = S.iters - 1;
+    if (D.group && iter > 0 && iter % kPruneEvery == 0) {
+        const double best = __longlong_as_double((long long)D.gbest[D.group[s]]);
+        if (isfinite(best) && S.sse > best * kPruneFactor) {
+            S.status = LM_PRUNED;
+            D.tmask[s] = 0;
+            return;
+        }
+    }
+    // J'J and J'r of the data rows, plus the Tikhonov rows' diagonal terms
+    double A[64], g[8];
+    for (int k = 0; k < dim * dim; ++k) A[k] = S.jtj[k];
+    for (int k = 0; k < dim; ++k) g[k] = S.grad[k];
+    if (D.prior) {
+        const double rw = sqrt(D.regw[s]);
+        const double w2 = rw * rw;
+        for (int k = 0; k < dim; ++k) {
+            const double jk = 1.0 / reg_scale(k);
+            const double r = (S.p[k] - D.prior[s * dim + k]) / reg_scale(k);
+            g[k] += (w2 * jk) * r;
+            A[k * dim + k] += (w2 * jk) * jk;
+        }
+    }
     double gn = 0.0;
-    for (int k = 0; k < dim; ++k) gn += S.grad[k] * S.grad[k];
+    for (int k = 0; k < dim; ++k) gn += g[k] * g[k];
     if (sqrt(gn) < kTolGrad) {
         S.status = LM_CONVERGED;
         D.tmask[s] = 0;
         return;
     }
-    lm_solve(S.jtj, S.grad, S.lam, dim, S.dp);
+    lm_solve(A, g, S.lam, dim, S.dp);
     for (int k = 0; k < dim; ++k) S.p_new[k] = S.p[k] + S.dp[k];
     if (!bounds_ok(S.p_new, dim)) {
         S.lam = fmin(S.lam * kLamUp, kLamMax);
@@ -289,7 +349,7 @@ __global__ void k_lm_accept(LMDev D) {
         const double t = D.w[i] * D.res_new[i];
         part += t * t;
     }
-    const double sse_new = warp_sum(part);
+    const double sse_new = add_reg_sse(D, s, S.p_new, warp_sum(part));
     const bool accept = sse_new < S.sse;
     if (accept)
         for (int64_t i = D.off[s] + lane; i < D.off[s + 1]; i += 32) D.res[i] = D.res_new[i];
@@ -301,6 +361,7 @@ __global__ void k_lm_accept(LMDev D) {
         for (int k = 0; k < dim; ++k) { S.p[k] = S.p_new[k]; D.pcur[s * dim + k] = S.p[k]; }
         S.sse = sse_new;
         S.lam = fmax(S.lam * kLamDown, 1e-12);
+        if (D.group) atomicMin(D.gbest + D.group[s], (unsigned long long)__double_as_longlong(sse_new));
         S.need_jac = 1;
         D.jmask[s] = 1;
         double sn = 0.0;
@@ -324,7 +385,7 @@ __global__ void k_lm_sse0(LMDev D) {
         part += t * t;
     }
     const double sse = warp_sum(part);
-    if (lane == 0) { D.st[s].sse = sse; D.tmask[s] = 0; }
+    if (lane == 0) { D.st[s].sse = add_reg_sse(D, s, D.st[s].p, sse); D.tmask[s] = 0; }
 }
 
 // Count surfaces still iterating and drive the graph's WHILE condition.
@@ -383,7 +444,7 @@ __global__ void k_lm_final(LMDev D, ope_calib_result* out) {
     for (int k = 0; k < dim; ++k) r.weakest_direction[k] = evec[weakest * dim + k];
     r.iters = S.iters;
     r.converged = S.status == LM_CONVERGED ? 1 : 0;
-    r.early_stopped = 0;
+    r.early_stopped = S.status == LM_PRUNED ? 1 : 0;
     r.status = S.status;
     out[s] = r;
 }
@@ -397,6 +458,7 @@ struct GraphCache {
     int model = -1, nq = -1, ns = -1;
     double tol = 0.0;
     cudaStream_t stream = nullptr;
+    bool prior = false, group = false;
 };
 }  // namespace
 
@@ -411,7 +473,7 @@ thread_local CalibGraph g_lm_graph;
 struct Layout {
     size_t total;
     size_t q, iv, w, off, sidx, st, pcur, ptrial, jmask, tmask, price, pgrad, res, res_new, jrow, counters, out,
-        scratch;
+        prior, regw, group, gbest, scratch;
 };
 
 Layout layout(size_t nq, size_t ns, int dim) {
@@ -435,6 +497,10 @@ Layout layout(size_t nq, size_t ns, int dim) {
     L.jrow = take(nq * dim * sizeof(double));
     L.counters = take(4 * sizeof(unsigned int));
     L.out = take(ns * sizeof(ope_calib_result));
+    L.prior = take(ns * dim * sizeof(double));
+    L.regw = take(ns * sizeof(double));
+    L.group = take(ns * sizeof(int32_t));
+    L.gbest = take(ns * sizeof(unsigned long long));
     L.scratch = take(grad_scratch_bytes(nq, dim));
     L.total = o;
     return L;
@@ -461,6 +527,10 @@ LMDev make_dev(char* base, const Layout& L, int nq, int ns, int dim) {
     D.res_new = reinterpret_cast<double*>(base + L.res_new);
     D.jrow = reinterpret_cast<double*>(base + L.jrow);
     D.counters = reinterpret_cast<unsigned int*>(base + L.counters);
+    D.prior = nullptr;
+    D.regw = nullptr;
+    D.group = nullptr;
+    D.gbest = nullptr;
     return D;
 }
 
@@ -545,7 +615,7 @@ size_t calib_pinned_bytes(size_t nq, size_t ns, int dim) {
 int calib_enqueue(int model, const ope_contract* quotes, const double* iv_market, const double* weights, size_t nq,
                   const int64_t* surf_offsets, const int64_t* off_h, size_t ns, const double* p0,
                   ope_calib_result* out, double tol, cudaMemcpyKind kind, cudaMemcpyKind out_kind, char* dev,
-                  char* pin, cudaStream_t st, CalibGraph* G) {
+                  char* pin, cudaStream_t st, CalibGraph* G, const CalibExtra* ex) {
     ThreadCtx& c = tctx();
     const int dim = param_stride(model);
     const Layout L = layout(nq, ns, dim);
@@ -577,6 +647,29 @@ int calib_enqueue(int model, const ope_contract* quotes, const double* iv_market
         p0_dev = reinterpret_cast<const double*>(base + L.ptrial);
     }
     LMDev D = make_dev(base, L, (int)nq, (int)ns, dim);
+    if (ex && ex->prior) {
+        if (!ex->reg_weight) return set_error(OPE_ERR_INVALID_ARG, "a prior needs its reg_weight");
+        OPE_CHECK(cudaMemcpyAsync(base + L.prior, ex->prior, ns * dim * sizeof(double), cudaMemcpyHostToDevice, st));
+        OPE_CHECK(cudaMemcpyAsync(base + L.regw, ex->reg_weight, ns * sizeof(double), cudaMemcpyHostToDevice, st));
+        D.prior = reinterpret_cast<const double*>(base + L.prior);
+        D.regw = reinterpret_cast<const double*>(base + L.regw);
+    }
+    if (ex && ex->group) {
+        if (ex->n_group < 1 || (size_t)ex->n_group > ns) return set_error(OPE_ERR_INVALID_ARG, "bad restart group count");
+        for (size_t s = 0; s < ns; ++s)
+            if (ex->group[s] < 0 || ex->group[s] >= ex->n_group) return set_error(OPE_ERR_INVALID_ARG, "bad restart group");
+        std::vector<unsigned long long> gb(ex->n_group);
+        for (int g = 0; g < ex->n_group; ++g) {
+            const double v = ex->gbest0 ? ex->gbest0[g] : __builtin_inf();
+            if (!(v >= 0.0)) return set_error(OPE_ERR_INVALID_ARG, "shared best SSE must be >= 0");
+            std::memcpy(&gb[g], &v, sizeof(double));
+        }
+        OPE_CHECK(cudaMemcpyAsync(base + L.group, ex->group, ns * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+        OPE_CHECK(cudaMemcpyAsync(base + L.gbest, gb.data(), gb.size() * sizeof(unsigned long long),
+                                  cudaMemcpyHostToDevice, st));
+        D.group = reinterpret_cast<const int32_t*>(base + L.group);
+        D.gbest = reinterpret_cast<unsigned long long*>(base + L.gbest);
+    }
     // initial state and residuals at p0 (calibration.rs:472-475)
     k_lm_init<<<((int)ns + 127) / 128, 128, 0, st>>>(D, p0_dev);
     OPE_CHECK(cudaGetLastError());
@@ -590,8 +683,9 @@ int calib_enqueue(int model, const ope_contract* quotes, const double* iv_market
     c.launches += 3;
     // the LM loop: one conditional-WHILE graph launch
     GraphCache& g = G->cache;
+    const bool has_prior = D.prior != nullptr, has_group = D.group != nullptr;
     if (!(g.exec && g.ws == dev && g.model == model && g.nq == (int)nq && g.ns == (int)ns && g.tol == tol &&
-          g.stream == st)) {
+          g.stream == st && g.prior == has_prior && g.group == has_group)) {
         OPE_TRY(build_graph(model, D, base, L, tol, st, g));
         g.ws = dev;
         g.model = model;
@@ -599,6 +693,8 @@ int calib_enqueue(int model, const ope_contract* quotes, const double* iv_market
         g.ns = (int)ns;
         g.tol = tol;
         g.stream = st;
+        g.prior = has_prior;
+        g.group = has_group;
     }
     OPE_CHECK(cudaGraphLaunch(g.exec, st));
     // final Jacobian at the last accepted parameters, diagnostics
@@ -627,7 +723,7 @@ void calib_graph_release(CalibGraph* G) {
 
 int run_calibration(int model, const ope_contract* quotes, const double* iv_market, const double* weights, size_t nq,
                     const int64_t* surf_offsets, size_t ns, const double* p0, ope_calib_result* out, double tol,
-                    bool device_ptrs, cudaStream_t ust) {
+                    bool device_ptrs, cudaStream_t ust, const CalibExtra* ex) {
     ThreadCtx& c = tctx();
     const int dim = param_stride(model);
     void* ws;
@@ -646,7 +742,7 @@ int run_calibration(int model, const ope_contract* quotes, const double* iv_mark
     const cudaMemcpyKind kind = device_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     OPE_TRY(calib_enqueue(model, quotes, iv_market, weights, nq, surf_offsets, off_h.data(), ns, p0, out, tol, kind,
                           device_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, static_cast<char*>(ws),
-                          static_cast<char*>(pin), st, &g_lm_graph));
+                          static_cast<char*>(pin), st, &g_lm_graph, ex));
     // the pinned staging is reused by the next call: wait for this one's copies
     OPE_CHECK(cudaStreamSynchronize(st));
     return OPE_OK;

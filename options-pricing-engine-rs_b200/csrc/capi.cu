@@ -282,6 +282,62 @@ int ope_calibrate_surfaces(int32_t model, const ope_contract* quotes, const doub
                            device_ptrs(opts), user_stream(opts));
 }
 
+int ope_calibrate_surfaces_reg(int32_t model, const ope_contract* quotes, const double* iv_market,
+                               const double* weights, size_t n_quotes, const int64_t* surf_offsets, size_t n_surf,
+                               const double* p0, const double* prior, const double* reg_weight,
+                               ope_calib_result* out, const ope_options* opts) {
+    OPE_TRY(check_model(model));
+    double tol;
+    OPE_TRY(resolve_tol(opts, &tol));
+    if (n_surf == 0) return OPE_OK;
+    if (!quotes || !iv_market || !surf_offsets || !p0 || !out || !prior || !reg_weight)
+        return set_error(OPE_ERR_INVALID_ARG, "NULL argument");
+    if (n_quotes == 0) return set_error(OPE_ERR_INVALID_ARG, "nothing to calibrate");  // calibration.rs:438
+    for (size_t s = 0; s < n_surf; ++s)
+        if (!(reg_weight[s] >= 0.0)) return set_error(OPE_ERR_INVALID_ARG, "reg_weight must be >= 0");
+    OPE_TRY(ensure_device());
+    CalibExtra ex;
+    ex.prior = prior;
+    ex.reg_weight = reg_weight;
+    return run_calibration(model, quotes, iv_market, weights, n_quotes, surf_offsets, n_surf, p0, out, tol,
+                           device_ptrs(opts), user_stream(opts), &ex);
+}
+
+int ope_calibrate_multistart(int32_t model, const ope_contract* quotes, const double* iv_market,
+                             const double* weights, size_t n_quotes, const int64_t* surf_offsets, size_t n_surf,
+                             const double* p0, int32_t n_restarts, uint64_t seed, const double* shared_best0,
+                             ope_multistart_result* out, ope_calib_result* out_restarts, const ope_options* opts) {
+    OPE_TRY(check_model(model));
+    double tol;
+    OPE_TRY(resolve_tol(opts, &tol));
+    if (n_surf == 0) return OPE_OK;
+    if (!quotes || !iv_market || !surf_offsets || !p0 || !out) return set_error(OPE_ERR_INVALID_ARG, "NULL argument");
+    if (device_ptrs(opts)) return set_error(OPE_ERR_INVALID_ARG, "ope_calibrate_multistart takes host pointers");
+    if (n_quotes == 0) return set_error(OPE_ERR_INVALID_ARG, "nothing to calibrate");
+    OPE_TRY(ensure_device());
+    return run_multistart(model, quotes, iv_market, weights, n_quotes, surf_offsets, n_surf, p0, n_restarts, seed,
+                          shared_best0, out, out_restarts, tol);
+}
+
+int ope_calibrate_global(int32_t model, const ope_contract* quotes, const double* iv_market, const double* weights,
+                         size_t n_quotes, const int64_t* surf_offsets, size_t n_surf, int32_t n_pop, int32_t n_gen,
+                         uint64_t seed, const double* prior, const double* reg_weight, ope_global_result* out,
+                         const ope_options* opts) {
+    OPE_TRY(check_model(model));
+    double tol;
+    OPE_TRY(resolve_tol(opts, &tol));
+    if (n_surf == 0) return OPE_OK;
+    if (!quotes || !iv_market || !surf_offsets || !out) return set_error(OPE_ERR_INVALID_ARG, "NULL argument");
+    if (device_ptrs(opts)) return set_error(OPE_ERR_INVALID_ARG, "ope_calibrate_global takes host pointers");
+    if (n_quotes == 0) return set_error(OPE_ERR_INVALID_ARG, "nothing to calibrate");
+    if (prior)
+        for (size_t s = 0; s < n_surf; ++s)
+            if (!reg_weight || !(reg_weight[s] >= 0.0)) return set_error(OPE_ERR_INVALID_ARG, "reg_weight must be >= 0");
+    OPE_TRY(ensure_device());
+    return run_global(model, quotes, iv_market, weights, n_quotes, surf_offsets, n_surf, n_pop, n_gen, seed, prior,
+                      reg_weight, out, tol);
+}
+
 int ope_calib_jacobian(int32_t model, const ope_contract* quotes, const double* iv_market, size_t n_quotes,
                        const int64_t* surf_offsets, size_t n_surf, const double* params, double* out_jac,
                        double* out_res, const ope_options* opts) {

@@ -77,18 +77,38 @@ int launch_price_grad(int model, const ope_contract* con, size_t n, const int64_
                       double* out_grad, void* scratch, cudaStream_t st, const int32_t* surf_mask = nullptr);
 // Batched LM calibration (calib.cu).
 struct CalibGraph;  // an instantiated LM graph (one per stream of use)
+// Optional parts of calibrate_inner for a calibration batch (host pointers).
+// prior / reg_weight: per surface, a Tikhonov pull toward prior[s] (ns x dim)
+// with weight reg_weight[s] (calibration.rs:448-470).  group: per surface, a
+// restart group in [0, n_group) whose members share a best SSE and prune
+// against it (calibration.rs:482-490, 520-523); gbest0: n_group initial shared
+// best values (NULL: +inf).
+struct CalibExtra {
+    const double* prior = nullptr;
+    const double* reg_weight = nullptr;
+    const int32_t* group = nullptr;
+    const double* gbest0 = nullptr;
+    int n_group = 0;
+};
 size_t calib_workspace_bytes(size_t nq, size_t ns, int dim);
 size_t calib_pinned_bytes(size_t nq, size_t ns, int dim);
 int calib_enqueue(int model, const ope_contract* quotes, const double* iv_market, const double* weights, size_t nq,
                   const int64_t* surf_offsets, const int64_t* off_h, size_t ns, const double* p0,
                   ope_calib_result* out, double tol, cudaMemcpyKind kind, cudaMemcpyKind out_kind, char* dev,
-                  char* pin, cudaStream_t st, CalibGraph* G);
+                  char* pin, cudaStream_t st, CalibGraph* G, const CalibExtra* ex = nullptr);
 CalibGraph* calib_graph_new();
 void calib_graph_release(CalibGraph* G);
 void calib_graph_delete(CalibGraph* G);
 int run_calibration(int model, const ope_contract* quotes, const double* iv_market, const double* weights, size_t nq,
                     const int64_t* surf_offsets, size_t ns, const double* p0, ope_calib_result* out, double tol,
-                    bool device_ptrs, cudaStream_t st);
+                    bool device_ptrs, cudaStream_t st, const CalibExtra* ex = nullptr);
+// Multistart and differential-evolution calibration (calib_global.cu), host pointers.
+int run_multistart(int model, const ope_contract* quotes, const double* iv_market, const double* weights, size_t nq,
+                   const int64_t* surf_offsets, size_t ns, const double* p0, int n_restarts, uint64_t seed,
+                   const double* shared_best0, ope_multistart_result* out, ope_calib_result* out_restarts, double tol);
+int run_global(int model, const ope_contract* quotes, const double* iv_market, const double* weights, size_t nq,
+               const int64_t* surf_offsets, size_t ns, int n_pop, int n_gen, uint64_t seed, const double* prior,
+               const double* reg_weight, ope_global_result* out, double tol);
 int run_calib_jacobian(int model, const ope_contract* quotes, const double* iv_market, size_t nq,
                        const int64_t* surf_offsets, size_t ns, const double* params, double* out_jac,
                        double* out_res, double tol);

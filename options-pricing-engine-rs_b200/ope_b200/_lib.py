@@ -76,6 +76,12 @@ _sig("ope_price_gradient_surfaces", ctypes.c_int,
 _sig("ope_selftest_math", ctypes.c_int, [ctypes.POINTER(_u64), ctypes.POINTER(_u64)])
 _sig("ope_calibrate_surfaces", ctypes.c_int,
      [_i32, _vp, _vp, _vp, _sz, _vp, _sz, _vp, _vp, ctypes.POINTER(Options)])
+_sig("ope_calibrate_surfaces_reg", ctypes.c_int,
+     [_i32, _vp, _vp, _vp, _sz, _vp, _sz, _vp, _vp, _vp, _vp, ctypes.POINTER(Options)])
+_sig("ope_calibrate_multistart", ctypes.c_int,
+     [_i32, _vp, _vp, _vp, _sz, _vp, _sz, _vp, _i32, _u64, _vp, _vp, _vp, ctypes.POINTER(Options)])
+_sig("ope_calibrate_global", ctypes.c_int,
+     [_i32, _vp, _vp, _vp, _sz, _vp, _sz, _i32, _i32, _u64, _vp, _vp, _vp, ctypes.POINTER(Options)])
 _sig("ope_calib_jacobian", ctypes.c_int, [_i32, _vp, _vp, _sz, _vp, _sz, _vp, _vp, _vp, ctypes.POINTER(Options)])
 _sig("ope_batch_implied_vol", ctypes.c_int, [_vp, _sz, _vp, _vp, _vp, ctypes.POINTER(Options)])
 _sig("ope_server_create", ctypes.c_int, [_vp, _vp])

@@ -267,6 +267,148 @@ def calibrate_bates(quotes, iv_market, p0, weights=None, tol=REF_TOL):
         _params_array(p0, MODEL_BATES)), weights, tol)[0]
 
 
+MULTISTART_RESULT_DTYPE = np.dtype([
+    ("best", CALIB_RESULT_DTYPE), ("n_restarts", "<i4"), ("n_converged", "<i4"), ("n_pruned", "<i4"),
+    ("best_restart", "<i4"),
+])  # include/ope.h ope_multistart_result = calibration.rs:70-76 MultistartResult
+
+GLOBAL_RESULT_DTYPE = np.dtype([
+    ("best", CALIB_RESULT_DTYPE), ("de_best_sse", "<f8"), ("de_generations", "<i4"), ("n_pop", "<i4"),
+])  # include/ope.h ope_global_result = calibration.rs:296-300 GlobalCalibResult
+
+
+def _calib_inputs(model, quotes, iv_market, surf_offsets, weights):
+    con = contracts_array(quotes)
+    iv = np.ascontiguousarray(iv_market, dtype=np.float64)
+    off = np.ascontiguousarray(surf_offsets, dtype=np.int64)
+    if iv.size != con.size:
+        raise ValueError("iv_market must have one entry per quote")
+    w = None if weights is None else np.ascontiguousarray(weights, dtype=np.float64)
+    return con, iv, off, w
+
+
+def _per_surface(x, n_surf, model, name):
+    p = _params_array(x, model)
+    if p.ndim == 1:
+        p = np.ascontiguousarray(np.broadcast_to(p, (n_surf, p.size)))
+    if p.shape[0] != n_surf:
+        raise ValueError(f"{name} must be (n_surf, 5|8)")
+    return p
+
+
+def calibrate_surfaces_reg(model: int, quotes, iv_market, surf_offsets, p0, prior, reg_weight, weights=None,
+                           tol=REF_TOL) -> np.ndarray:
+    """LM with a Tikhonov pull toward `prior` (calibration.rs:220-230), many surfaces at once."""
+    con, iv, off, w = _calib_inputs(model, quotes, iv_market, surf_offsets, weights)
+    n_surf = off.size - 1
+    p = _per_surface(p0, n_surf, model, "p0")
+    pr = _per_surface(prior, n_surf, model, "prior")
+    rw = np.ascontiguousarray(np.broadcast_to(np.asarray(reg_weight, np.float64), (n_surf,)))
+    out = np.zeros(n_surf, dtype=CALIB_RESULT_DTYPE)
+    o = _opts(tol)
+    check(load().ope_calibrate_surfaces_reg(model, con.ctypes.data, iv.ctypes.data,
+                                            None if w is None else w.ctypes.data, con.size, off.ctypes.data, n_surf,
+                                            p.ctypes.data, pr.ctypes.data, rw.ctypes.data, out.ctypes.data,
+                                            ctypes.byref(o)))
+    return out
+
+
+def calibrate_multistart(model: int, quotes, iv_market, surf_offsets, p0, n_restarts: int, seed: int, weights=None,
+                         shared_best0=None, return_restarts: bool = False, tol=REF_TOL):
+    """calibration.rs:246-314 for many surfaces at once.  Returns MULTISTART_RESULT_DTYPE
+    records (and, with return_restarts, every restart's CALIB_RESULT_DTYPE record,
+    shape (n_surf, max(n_restarts, 1)))."""
+    con, iv, off, w = _calib_inputs(model, quotes, iv_market, surf_offsets, weights)
+    n_surf = off.size - 1
+    p = _per_surface(p0, n_surf, model, "p0")
+    nr = max(int(n_restarts), 1)
+    out = np.zeros(n_surf, dtype=MULTISTART_RESULT_DTYPE)
+    allr = np.zeros((n_surf, nr), dtype=CALIB_RESULT_DTYPE) if return_restarts else None
+    sb = None if shared_best0 is None else np.ascontiguousarray(
+        np.broadcast_to(np.asarray(shared_best0, np.float64), (n_surf,)))
+    o = _opts(tol)
+    check(load().ope_calibrate_multistart(model, con.ctypes.data, iv.ctypes.data,
+                                          None if w is None else w.ctypes.data, con.size, off.ctypes.data, n_surf,
+                                          p.ctypes.data, int(n_restarts), ctypes.c_uint64(int(seed) & (2**64 - 1)),
+                                          None if sb is None else sb.ctypes.data, out.ctypes.data,
+                                          None if allr is None else allr.ctypes.data, ctypes.byref(o)))
+    return (out, allr) if return_restarts else out
+
+
+def calibrate_global(model: int, quotes, iv_market, surf_offsets, n_pop: int, n_gen: int, seed: int, weights=None,
+                     prior=None, reg_weight=None, tol=REF_TOL) -> np.ndarray:
+    """calibration.rs:316-427 (differential evolution + LM polish, regularised when
+    `prior` is given) for many surfaces at once; GLOBAL_RESULT_DTYPE records."""
+    con, iv, off, w = _calib_inputs(model, quotes, iv_market, surf_offsets, weights)
+    n_surf = off.size - 1
+    pr = rw = None
+    if prior is not None:
+        pr = _per_surface(prior, n_surf, model, "prior")
+        rw = np.ascontiguousarray(np.broadcast_to(np.asarray(reg_weight, np.float64), (n_surf,)))
+    out = np.zeros(n_surf, dtype=GLOBAL_RESULT_DTYPE)
+    o = _opts(tol)
+    check(load().ope_calibrate_global(model, con.ctypes.data, iv.ctypes.data, None if w is None else w.ctypes.data,
+                                      con.size, off.ctypes.data, n_surf, int(n_pop), int(n_gen),
+                                      ctypes.c_uint64(int(seed) & (2**64 - 1)),
+                                      None if pr is None else pr.ctypes.data, None if rw is None else rw.ctypes.data,
+                                      out.ctypes.data, ctypes.byref(o)))
+    return out
+
+
+def _one(model, quotes):
+    return [0, len(quotes)]
+
+
+def calibrate_heston_regularized(quotes, iv_market, p0, prior, reg_weight, weights=None, tol=REF_TOL):
+    """calibration.rs:220-224 (one surface)."""
+    return calibrate_surfaces_reg(MODEL_HESTON, quotes, iv_market, _one(0, iv_market), p0, prior, reg_weight,
+                                  weights, tol)[0]
+
+
+def calibrate_bates_regularized(quotes, iv_market, p0, prior, reg_weight, weights=None, tol=REF_TOL):
+    """calibration.rs:226-230 (one surface)."""
+    return calibrate_surfaces_reg(MODEL_BATES, quotes, iv_market, _one(1, iv_market), p0, prior, reg_weight,
+                                  weights, tol)[0]
+
+
+def calibrate_heston_multistart(quotes, iv_market, p0, n_restarts, seed, weights=None, tol=REF_TOL):
+    """calibration.rs:246-250 (one surface)."""
+    return calibrate_multistart(MODEL_HESTON, quotes, iv_market, _one(0, iv_market), p0, n_restarts, seed,
+                                weights, tol=tol)[0]
+
+
+def calibrate_bates_multistart(quotes, iv_market, p0, n_restarts, seed, weights=None, tol=REF_TOL):
+    """calibration.rs:252-256 (one surface)."""
+    return calibrate_multistart(MODEL_BATES, quotes, iv_market, _one(1, iv_market), p0, n_restarts, seed,
+                                weights, tol=tol)[0]
+
+
+def calibrate_heston_global(quotes, iv_market, n_pop, n_gen, seed, weights=None, tol=REF_TOL):
+    """calibration.rs:316-320 (one surface)."""
+    return calibrate_global(MODEL_HESTON, quotes, iv_market, _one(0, iv_market), n_pop, n_gen, seed, weights,
+                            tol=tol)[0]
+
+
+def calibrate_bates_global(quotes, iv_market, n_pop, n_gen, seed, weights=None, tol=REF_TOL):
+    """calibration.rs:322-326 (one surface)."""
+    return calibrate_global(MODEL_BATES, quotes, iv_market, _one(1, iv_market), n_pop, n_gen, seed, weights,
+                            tol=tol)[0]
+
+
+def calibrate_heston_global_regularized(quotes, iv_market, n_pop, n_gen, seed, prior, reg_weight, weights=None,
+                                        tol=REF_TOL):
+    """calibration.rs:335-340 (one surface)."""
+    return calibrate_global(MODEL_HESTON, quotes, iv_market, _one(0, iv_market), n_pop, n_gen, seed, weights,
+                            prior, reg_weight, tol)[0]
+
+
+def calibrate_bates_global_regularized(quotes, iv_market, n_pop, n_gen, seed, prior, reg_weight, weights=None,
+                                       tol=REF_TOL):
+    """calibration.rs:342-347 (one surface)."""
+    return calibrate_global(MODEL_BATES, quotes, iv_market, _one(1, iv_market), n_pop, n_gen, seed, weights,
+                            prior, reg_weight, tol)[0]
+
+
 def calib_jacobian(model: int, quotes, iv_market, surf_offsets, params, tol=REF_TOL):
     """The device IV-space Jacobian (n x dim) and IV residuals at params (calibration.rs:613-652)."""
     con = contracts_array(quotes)
@@ -341,4 +483,8 @@ __all__ = [
     "price_surfaces", "price_surfaces_device", "batch_price_device", "contracts_array", "REF_TOL",
     "MODEL_HESTON", "MODEL_BATES", "RESULT_DTYPE", "kernel_launch_count", "device_info", "measure_fp64_peak", "price_gradient_surfaces",
     "CALIB_RESULT_DTYPE", "batch_implied_vol", "calibrate_surfaces", "calibrate_heston", "calibrate_bates", "calib_jacobian",
+    "MULTISTART_RESULT_DTYPE", "GLOBAL_RESULT_DTYPE", "calibrate_surfaces_reg", "calibrate_multistart",
+    "calibrate_global", "calibrate_heston_regularized", "calibrate_bates_regularized", "calibrate_heston_multistart",
+    "calibrate_bates_multistart", "calibrate_heston_global", "calibrate_bates_global",
+    "calibrate_heston_global_regularized", "calibrate_bates_global_regularized",
 ]

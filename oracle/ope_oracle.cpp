@@ -934,52 +934,122 @@ struct CalibOut {
     int32_t iters, converged, early_stopped, pad;
 };
 
-// calibration.rs:433-569 (no multistart pruning: shared_best_sse = None)
-CalibOut calibrate_inner(const Model& m, const Quote* q, int n, const double* p0, const double* prior,
-                         double reg_weight) {
-    const int MAX_ITER = 200;
-    const double TOL_GRAD = 1e-8, TOL_PARAMS = 1e-10, LM_INIT = 1e-3, LM_UP = 10.0, LM_DOWN = 0.1,
-                 LM_MAX = 1e8;
+// The device LM's Jacobian restated on the CPU (not the reference's): every
+// column exact, d iv / d p = (d price / d p by forward-mode AD) / BSM vega at
+// the model IV, and a zero row where that IV solve fails or |vega| < 1e-10.
+// The reference (jacobian above) uses central differences for the Heston
+// columns; this variant lets a test follow the device LM iteration for
+// iteration.
+void jacobian_exact(const Model& m, const Quote* q, int n, const double* p, double* j) {
     int dim = m.dim;
-    bool reg = prior != nullptr;
-    int rows = n + (reg ? dim : 0);
-    std::vector<double> base_w(n);
-    for (int i = 0; i < n; ++i) base_w[i] = q[i].weight;
-    auto aug_res = [&](const double* pv, double* res, double* w) {
-        residuals(m, q, n, pv, res);
-        for (int i = 0; i < n; ++i) w[i] = base_w[i];
-        if (reg) {
-            double rw = std::sqrt(reg_weight);
-            for (int i = 0; i < dim; ++i) { res[n + i] = (pv[i] - prior[i]) / m.reg_scale(i); w[n + i] = rw; }
+    Heston h{p[0], p[1], p[2], p[3], p[4]};
+    bool bates = dim == 8;
+    for (int row = 0; row < n; ++row) {
+        const Contract& c = q[row].c;
+        double* jr = j + (size_t)row * dim;
+        double px = m.price(p, c);
+        double iv, vega = 0.0;
+        bool ok = implied_vol(with_vol(c, q[row].iv_market), px, &iv);
+        if (ok) vega = bsm_price_and_greeks(with_vol(c, iv)).vega;
+        if (!ok || std::fabs(vega) < 1e-10) {
+            for (int k = 0; k < dim; ++k) jr[k] = 0.0;
+            continue;
         }
-    };
-    auto aug_jac = [&](const double* pv, double* j) {
-        jacobian(m, q, n, pv, j);
-        if (reg)
+        JumpSpec js = bates ? JumpSpec{1, p[5], p[6], p[7], -1} : JumpSpec{0, 0, 0, 0, -1};
+        for (int a = 0; a < 5; ++a) {
+            double pv, dv;
+            forward_pass(c.spot, c.strike, c.expiry, c.rate, c.div_yield, h, c.opt_type, a, js, REF_TOL, &pv, &dv);
+            jr[a] = dv / vega;
+        }
+        for (int a = 0; bates && a < 3; ++a) {
+            double pv, dv;
+            JumpSpec ja{2, p[5], p[6], p[7], a};
+            forward_pass(c.spot, c.strike, c.expiry, c.rate, c.div_yield, h, c.opt_type, -1, ja, REF_TOL, &pv, &dv);
+            jr[5 + a] = dv / vega;
+        }
+    }
+}
+
+// calibration.rs:433-569 as a resumable state machine: init() is the set-up
+// (lines 438-479), step() one pass of the iteration loop (481-538), finish()
+// the data-only diagnostics (541-568).  Running step() until done() is
+// exactly calibrate_inner; multistart runs several machines in lockstep.
+// prior == nullptr: no Tikhonov rows (calibration.rs:448-470).  jac_mode 0:
+// the reference's Jacobian; 1: jacobian_exact.
+struct LMRun {
+    static constexpr int MAX_ITER = 200;                                          // calibration.rs:30
+    static constexpr double TOL_GRAD = 1e-8, TOL_PARAMS = 1e-10, LM_INIT = 1e-3,  // calibration.rs:31-36
+        LM_UP = 10.0, LM_DOWN = 0.1, LM_MAX = 1e8, PRUNE_FACTOR = 8.0;           // calibration.rs:263
+    static constexpr int PRUNE_CHECK_EVERY = 10;                                  // calibration.rs:264
+
+    const Model* m = nullptr;
+    const Quote* q = nullptr;
+    int n = 0, dim = 0, rows = 0, jac_mode = 0;
+    const double* prior = nullptr;
+    double reg_weight = 0.0;
+    std::vector<double> base_w, res, w, res_new, w_new, j;
+    double p[8] = {0};
+    double lam = LM_INIT, sse = 0.0;
+    int iters = 0, iter = 0;
+    bool converged = false, early_stopped = false, finished = false;
+
+    void jac(const double* pv, double* jj) const {
+        if (jac_mode == 1) jacobian_exact(*m, q, n, pv, jj);
+        else jacobian(*m, q, n, pv, jj);
+    }
+    void aug_res(const double* pv, double* r, double* ww) const {
+        residuals(*m, q, n, pv, r);
+        for (int i = 0; i < n; ++i) ww[i] = base_w[i];
+        if (prior) {
+            double rw = std::sqrt(reg_weight);
+            for (int i = 0; i < dim; ++i) { r[n + i] = (pv[i] - prior[i]) / m->reg_scale(i); ww[n + i] = rw; }
+        }
+    }
+    void aug_jac(const double* pv, double* jj) const {
+        jac(pv, jj);
+        if (prior)
             for (int i = 0; i < dim; ++i)
-                for (int c = 0; c < dim; ++c) j[(size_t)(n + i) * dim + c] = (c == i) ? 1.0 / m.reg_scale(i) : 0.0;
-    };
-    double p[8];
-    for (int i = 0; i < dim; ++i) p[i] = p0[i];
-    double lam = LM_INIT;
-    std::vector<double> res(rows), w(rows), res_new(rows), w_new(rows), j((size_t)rows * dim);
-    aug_res(p, res.data(), w.data());
-    double sse = weighted_sse(res.data(), w.data(), rows);
-    int iters = 0;
-    bool converged = false;
-    for (int iter = 0; iter < MAX_ITER; ++iter) {
+                for (int c = 0; c < dim; ++c) jj[(size_t)(n + i) * dim + c] = (c == i) ? 1.0 / m->reg_scale(i) : 0.0;
+    }
+    void init(const Model& model, const Quote* quotes, int nq, const double* p0, const double* pr, double rw, int jm) {
+        m = &model; q = quotes; n = nq; dim = model.dim; prior = pr; reg_weight = rw; jac_mode = jm;
+        rows = n + (prior ? dim : 0);
+        base_w.resize(n);
+        for (int i = 0; i < n; ++i) base_w[i] = q[i].weight;
+        res.resize(rows); w.resize(rows); res_new.resize(rows); w_new.resize(rows); j.resize((size_t)rows * dim);
+        for (int i = 0; i < dim; ++i) p[i] = p0[i];
+        lam = LM_INIT;
+        aug_res(p, res.data(), w.data());
+        sse = weighted_sse(res.data(), w.data(), rows);
+    }
+    bool done() const { return finished || iter >= MAX_ITER; }
+    // One loop iteration.  prune: this run takes part in multistart pruning,
+    // against `shared_best` (the shared best SSE as it reads at the top of the
+    // iteration).  *accepted_sse receives the new SSE after an accepted step,
+    // else NaN (it is what the run would publish to the shared best).
+    void step(bool prune, double shared_best, double* accepted_sse) {
+        *accepted_sse = std::numeric_limits<double>::quiet_NaN();
+        if (done()) return;
         iters = iter + 1;
+        int this_iter = iter++;
+        if (prune && this_iter > 0 && this_iter % PRUNE_CHECK_EVERY == 0) {
+            if (std::isfinite(shared_best) && sse > shared_best * PRUNE_FACTOR) {
+                early_stopped = true;
+                finished = true;
+                return;
+            }
+        }
         aug_jac(p, j.data());
         double jtj[64], grad[8];
         jtj_and_grad(j.data(), rows, res.data(), w.data(), dim, jtj, grad);
         double gn = 0.0;
         for (int i = 0; i < dim; ++i) gn = gn + grad[i] * grad[i];
-        if (std::sqrt(gn) < TOL_GRAD) { converged = true; break; }
+        if (std::sqrt(gn) < TOL_GRAD) { converged = true; finished = true; return; }
         double dp[8];
         lm_step(jtj, grad, lam, dim, dp);
         double p_new[8];
         for (int i = 0; i < dim; ++i) p_new[i] = p[i] + dp[i];
-        if (!m.bounds_ok(p_new)) { lam = std::min(lam * LM_UP, LM_MAX); continue; }
+        if (!m->bounds_ok(p_new)) { lam = std::min(lam * LM_UP, LM_MAX); return; }
         aug_res(p_new, res_new.data(), w_new.data());
         double sse_new = weighted_sse(res_new.data(), w_new.data(), rows);
         if (sse_new < sse) {
@@ -988,40 +1058,166 @@ CalibOut calibrate_inner(const Model& m, const Quote* q, int n, const double* p0
             w.swap(w_new);
             sse = sse_new;
             lam = std::max(lam * LM_DOWN, 1e-12);
+            *accepted_sse = sse;
             double sn = 0.0;
             for (int i = 0; i < dim; ++i) sn = sn + dp[i] * dp[i];
-            if (std::sqrt(sn) < TOL_PARAMS) { converged = true; break; }
+            if (std::sqrt(sn) < TOL_PARAMS) { converged = true; finished = true; }
         } else {
             lam = std::min(lam * LM_UP, LM_MAX);
-            if (lam >= LM_MAX) break;
+            if (lam >= LM_MAX) finished = true;
         }
     }
-    CalibOut o{};
-    for (int i = 0; i < dim; ++i) o.params[i] = p[i];
-    std::vector<double> rd(n);
-    residuals(m, q, n, p, rd.data());
-    double wsum = 0.0;
-    for (int i = 0; i < n; ++i) wsum = wsum + base_w[i] * base_w[i];
-    o.rmse = std::sqrt(weighted_sse(rd.data(), base_w.data(), n) / wsum);
-    double mx = 0.0;
-    for (int i = 0; i < n; ++i) mx = std::fmax(mx, std::fabs(rd[i]));
-    o.max_err = mx;
-    std::vector<double> fj((size_t)n * dim);
-    jacobian(m, q, n, p, fj.data());
-    double jtj[64], grad[8], ev[8], evec[64];
-    jtj_and_grad(fj.data(), n, rd.data(), base_w.data(), dim, jtj, grad);
-    jacobi_eigen(jtj, dim, ev, evec);
-    double mx_e = -std::numeric_limits<double>::max(), mn_e = std::numeric_limits<double>::max();
-    for (int i = 0; i < dim; ++i) { mx_e = std::fmax(mx_e, ev[i]); mn_e = std::fmin(mn_e, ev[i]); }
-    o.condition_number = std::fabs(mn_e) > 1e-300 ? std::fabs(mx_e / mn_e) : INFINITY;
-    int weakest = 0;
-    for (int i = 1; i < dim; ++i)
-        if (total_key(std::fabs(ev[i])) < total_key(std::fabs(ev[weakest]))) weakest = i;  // min_by: first min
-    for (int k = 0; k < dim; ++k) o.weakest[k] = evec[weakest * dim + k];
-    o.iters = iters;
-    o.converged = converged ? 1 : 0;
-    o.early_stopped = 0;
-    return o;
+    CalibOut finish() const {
+        CalibOut o{};
+        for (int i = 0; i < dim; ++i) o.params[i] = p[i];
+        std::vector<double> rd(n);
+        residuals(*m, q, n, p, rd.data());
+        double wsum = 0.0;
+        for (int i = 0; i < n; ++i) wsum = wsum + base_w[i] * base_w[i];
+        o.rmse = std::sqrt(weighted_sse(rd.data(), base_w.data(), n) / wsum);
+        double mx = 0.0;
+        for (int i = 0; i < n; ++i) mx = std::fmax(mx, std::fabs(rd[i]));
+        o.max_err = mx;
+        std::vector<double> fj((size_t)n * dim);
+        jac(p, fj.data());
+        double jtj[64], grad[8], ev[8], evec[64];
+        jtj_and_grad(fj.data(), n, rd.data(), base_w.data(), dim, jtj, grad);
+        jacobi_eigen(jtj, dim, ev, evec);
+        double mx_e = -std::numeric_limits<double>::max(), mn_e = std::numeric_limits<double>::max();
+        for (int i = 0; i < dim; ++i) { mx_e = std::fmax(mx_e, ev[i]); mn_e = std::fmin(mn_e, ev[i]); }
+        o.condition_number = std::fabs(mn_e) > 1e-300 ? std::fabs(mx_e / mn_e) : INFINITY;
+        int weakest = 0;
+        for (int i = 1; i < dim; ++i)
+            if (total_key(std::fabs(ev[i])) < total_key(std::fabs(ev[weakest]))) weakest = i;  // min_by: first min
+        for (int k = 0; k < dim; ++k) o.weakest[k] = evec[weakest * dim + k];
+        o.iters = iters;
+        o.converged = converged ? 1 : 0;
+        o.early_stopped = early_stopped ? 1 : 0;
+        return o;
+    }
+};
+
+// calibration.rs:433-569.  shared_best: initial shared best SSE for a run
+// that takes part in pruning (calibration.rs:482-490); NaN: no pruning.
+CalibOut calibrate_inner(const Model& m, const Quote* q, int n, const double* p0, const double* prior,
+                         double reg_weight, int jac_mode = 0, double shared_best = NAN) {
+    LMRun r;
+    r.init(m, q, n, p0, prior, reg_weight, jac_mode);
+    const bool prune = !std::isnan(shared_best);
+    double acc;
+    while (!r.done()) {
+        r.step(prune, shared_best, &acc);
+        if (prune && acc < shared_best) shared_best = acc;
+    }
+    return r.finish();
+}
+
+// ---------------------------------------------------------------------------
+// rand 0.8 SmallRng + the samplers the calibration calls (calibration.rs:
+// 131-141, 179-185, 284, 372-392).  The reference lock file does not pin
+// rand (Cargo.toml:19 asks for 0.8 with small_rng), so this restates the
+// published 0.8.5 algorithms: SmallRng on 64-bit targets is xoshiro256++
+// (Blackman & Vigna), seeded by rand_core's default seed_from_u64 (PCG32);
+// gen::<f64>() = (next_u64 >> 11) * 2^-53; gen_range(lo..hi) on f64
+// draws v in [1,2) from the top 52 bits, res = (v - 1) * (hi - lo) + lo,
+// redrawn while res >= hi; gen_range(lo..hi) on usize is the widening-
+// multiply method with the (range << leading_zeros) - 1 rejection zone.
+// ---------------------------------------------------------------------------
+inline uint64_t splitmix64(uint64_t x) {  // mc.rs:337-343
+    x = x + 0x9E3779B97F4A7C15ull;
+    uint64_t z = x;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+struct SmallRng {
+    uint64_t s[4];
+    // xoshiro256++'s own seed_from_u64 (four SplitMix64 outputs); rand uses it
+    // only for an all-zero seed (Xoshiro256PlusPlus::from_seed).
+    static SmallRng xoshiro_seed_from_u64(uint64_t state) {
+        SmallRng r;
+        for (int k = 0; k < 4; ++k) {
+            state = state + 0x9e3779b97f4a7c15ull;
+            uint64_t z = state;
+            z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+            z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+            r.s[k] = z ^ (z >> 31);
+        }
+        return r;
+    }
+    // SmallRng::seed_from_u64 in rand 0.8 is rand_core 0.6's default
+    // SeedableRng::seed_from_u64 (SmallRng does not forward it to the inner
+    // generator): the 32-byte seed is eight PCG32 (XSH-RR) outputs, little
+    // endian, then Xoshiro256PlusPlus::from_seed.
+    static SmallRng seed_from_u64(uint64_t state) {
+        uint32_t x[8];
+        for (int k = 0; k < 8; ++k) {
+            state = state * 6364136223846793005ull + 11634580027462260723ull;
+            uint32_t xorshifted = (uint32_t)(((state >> 18) ^ state) >> 27);
+            uint32_t rot = (uint32_t)(state >> 59);
+            x[k] = (xorshifted >> rot) | (xorshifted << ((32 - rot) & 31));
+        }
+        SmallRng r;
+        for (int k = 0; k < 4; ++k) r.s[k] = (uint64_t)x[2 * k] | ((uint64_t)x[2 * k + 1] << 32);
+        if ((r.s[0] | r.s[1] | r.s[2] | r.s[3]) == 0) return xoshiro_seed_from_u64(0);
+        return r;
+    }
+    static uint64_t rotl(uint64_t x, int k) { return (x << k) | (x >> (64 - k)); }
+    uint64_t next_u64() {
+        uint64_t result = rotl(s[0] + s[3], 23) + s[0];
+        uint64_t t = s[1] << 17;
+        s[2] ^= s[0];
+        s[3] ^= s[1];
+        s[1] ^= s[2];
+        s[0] ^= s[3];
+        s[2] ^= t;
+        s[3] = rotl(s[3], 45);
+        return result;
+    }
+    double gen_f64() { return (double)(next_u64() >> 11) * (1.0 / 9007199254740992.0); }
+    double gen_range_f64(double lo, double hi) {
+        double scale = hi - lo;
+        for (;;) {
+            uint64_t bits = (next_u64() >> 12) | 0x3ff0000000000000ull;
+            double v12;
+            std::memcpy(&v12, &bits, 8);
+            double res = (v12 - 1.0) * scale + lo;
+            if (res < hi) return res;
+        }
+    }
+    uint64_t gen_range_usize(uint64_t lo, uint64_t hi) {  // [lo, hi)
+        uint64_t range = (hi - 1) - lo + 1;
+        if (range == 0) return next_u64();
+        uint64_t zone = (range << __builtin_clzll(range)) - 1;
+        for (;;) {
+            uint64_t v = next_u64();
+            unsigned __int128 mm = (unsigned __int128)v * range;
+            if ((uint64_t)mm <= zone) return lo + (uint64_t)(mm >> 64);
+        }
+    }
+};
+
+// calibration.rs:131-141 (Heston) and 179-185 (Bates)
+void random_guess(int dim, SmallRng& rng, double* v) {
+    double v0 = rng.gen_range_f64(0.005, 0.5);
+    double kappa = rng.gen_range_f64(0.3, 8.0);
+    double theta = rng.gen_range_f64(0.005, 0.5);
+    double sigma_cap = std::fmax(std::sqrt((2.0 * kappa) * theta) * 0.9, 0.05);
+    double sigma = rng.gen_range_f64(0.02, sigma_cap);
+    double rho = rng.gen_range_f64(-0.9, 0.9);
+    v[0] = v0; v[1] = kappa; v[2] = theta; v[3] = sigma; v[4] = rho;
+    if (dim == 8) {
+        v[5] = rng.gen_range_f64(0.0, 2.0);
+        v[6] = rng.gen_range_f64(-0.3, 0.1);
+        v[7] = rng.gen_range_f64(0.02, 0.4);
+    }
+}
+
+inline double rust_clamp(double x, double lo, double hi) {  // f64::clamp
+    if (x < lo) x = lo;
+    if (x > hi) x = hi;
+    return x;
 }
 
 inline int threads_or_default(int nthreads) {
@@ -1249,6 +1445,194 @@ void orc_calibrate(int dim, const void* contracts, const double* iv_market, cons
     Model m{dim};
     CalibOut o = calibrate_inner(m, q.data(), n, p0, prior, reg_weight);
     std::memcpy(out, &o, sizeof(o));
+}
+
+// One LM calibration with every option of calibrate_inner: Tikhonov prior
+// (calibration.rs:220-230; prior NULL = none), the Jacobian variant
+// (jac_mode, see LMRun) and a fixed shared best SSE to prune against
+// (calibration.rs:482-490; NaN = no pruning, as calibrate_heston does).
+void orc_calibrate_ex(int dim, const void* contracts, const double* iv_market, const double* weight, int n,
+                      const double* p0, const double* prior, double reg_weight, int jac_mode, double shared_best,
+                      void* out) {
+    const Contract* c = static_cast<const Contract*>(contracts);
+    std::vector<Quote> q(n);
+    for (int i = 0; i < n; ++i) q[i] = Quote{c[i], iv_market[i], weight ? weight[i] : 1.0};
+    Model m{dim};
+    CalibOut o = calibrate_inner(m, q.data(), n, p0, prior, reg_weight, jac_mode, shared_best);
+    std::memcpy(out, &o, sizeof(o));
+}
+
+// calibration.rs:246-314 calibrate_multistart.  Restart 0 starts at p0,
+// restart i at random_guess(SmallRng::seed_from_u64(splitmix64(seed ^ i))).
+// The reference runs restarts on rayon threads against a mutex-guarded
+// shared best, so which pruning checks see which updates depends on thread
+// timing.  Here the restarts advance in lockstep, one iteration each per
+// round, and every check of round k sees the updates of rounds < k: one of
+// the schedules the reference allows, and the one the device runs.
+// shared_best0: the shared best's initial value (the reference: +inf).
+// out_best: CalibOut of the lowest-RMSE restart (min_by: first minimum);
+// out_all (NULL or n_restarts records); counts = {n_converged, n_pruned,
+// index of the best restart}.
+void orc_calibrate_multistart(int dim, const void* contracts, const double* iv_market, const double* weight, int n,
+                              const double* p0, int n_restarts, uint64_t seed, int jac_mode, double shared_best0,
+                              void* out_best, void* out_all, int32_t* counts, int nthreads) {
+    const Contract* c = static_cast<const Contract*>(contracts);
+    std::vector<Quote> q(n);
+    for (int i = 0; i < n; ++i) q[i] = Quote{c[i], iv_market[i], weight ? weight[i] : 1.0};
+    Model m{dim};
+    const int nr = std::max(n_restarts, 1);
+    std::vector<double> starts((size_t)nr * dim);
+    for (int i = 0; i < nr; ++i) {
+        double* v = starts.data() + (size_t)i * dim;
+        if (i == 0) {
+            for (int k = 0; k < dim; ++k) v[k] = p0[k];
+        } else {
+            SmallRng rng = SmallRng::seed_from_u64(splitmix64(seed ^ (uint64_t)i));
+            random_guess(dim, rng, v);
+        }
+    }
+    std::vector<LMRun> runs(nr);
+    int nt = threads_or_default(nthreads);
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nt)
+    for (int i = 0; i < nr; ++i) runs[i].init(m, q.data(), n, starts.data() + (size_t)i * dim, nullptr, 0.0, jac_mode);
+    double shared = shared_best0;
+    std::vector<double> acc(nr);
+    for (;;) {
+        bool any = false;
+        for (int i = 0; i < nr; ++i) any = any || !runs[i].done();
+        if (!any) break;
+        const double snap = shared;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nt)
+        for (int i = 0; i < nr; ++i) runs[i].step(true, snap, &acc[i]);
+        for (int i = 0; i < nr; ++i)
+            if (acc[i] < shared) shared = acc[i];
+    }
+    std::vector<CalibOut> res(nr);
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nt)
+    for (int i = 0; i < nr; ++i) res[i] = runs[i].finish();
+    int best = 0, n_conv = 0, n_pruned = 0;
+    for (int i = 0; i < nr; ++i) {
+        n_conv += res[i].converged;
+        n_pruned += res[i].early_stopped;
+        if (total_key(res[i].rmse) < total_key(res[best].rmse)) best = i;
+    }
+    std::memcpy(out_best, &res[best], sizeof(CalibOut));
+    if (out_all) std::memcpy(out_all, res.data(), sizeof(CalibOut) * nr);
+    counts[0] = n_conv;
+    counts[1] = n_pruned;
+    counts[2] = best;
+}
+
+// calibration.rs:349-427 calibrate_global: DE/rand/1/bin (F 0.6, CR 0.9,
+// calibration.rs:324-325) over the parameter box, then one LM polish from
+// the DE winner, regularised toward prior when prior != NULL
+// (calibration.rs:335-347).  out: CalibOut of the polish; *de_best_sse the
+// winner's SSE; pop_out / fit_out (NULL or n_pop_used x dim / n_pop_used):
+// the final population and its fitness; *n_pop_used = max(n_pop, 4 dim).
+void orc_calibrate_global(int dim, const void* contracts, const double* iv_market, const double* weight, int n,
+                          int n_pop, int n_gen, uint64_t seed, const double* prior, double reg_weight, int jac_mode,
+                          void* out, double* de_best_sse, double* pop_out, double* fit_out, int32_t* n_pop_used,
+                          int nthreads) {
+    const Contract* c = static_cast<const Contract*>(contracts);
+    std::vector<Quote> q(n);
+    for (int i = 0; i < n; ++i) q[i] = Quote{c[i], iv_market[i], weight ? weight[i] : 1.0};
+    Model m{dim};
+    const int np = std::max(n_pop, 4 * dim);
+    std::vector<double> base_w(n);
+    for (int i = 0; i < n; ++i) base_w[i] = q[i].weight;
+    auto sse_of = [&](const double* v) -> double {
+        if (!m.bounds_ok(v)) return INFINITY;
+        std::vector<double> r(n);
+        residuals(m, q.data(), n, v, r.data());
+        return weighted_sse(r.data(), base_w.data(), n);
+    };
+    double lo[8], hi[8];
+    for (int d = 0; d < dim; ++d) m.bounds(d, &lo[d], &hi[d]);
+    SmallRng init_rng = SmallRng::seed_from_u64(splitmix64(seed));
+    std::vector<double> pop((size_t)np * dim), fit(np);
+    for (int i = 0; i < np; ++i) {
+        double* v = pop.data() + (size_t)i * dim;
+        bool got = false;
+        for (int attempt = 0; attempt < 20 && !got; ++attempt) {
+            for (int d = 0; d < dim; ++d) v[d] = init_rng.gen_range_f64(lo[d], hi[d]);
+            got = std::isfinite(sse_of(v));
+        }
+        if (!got)
+            for (int d = 0; d < dim; ++d) v[d] = init_rng.gen_range_f64(lo[d], hi[d]);
+    }
+    int nt = threads_or_default(nthreads);
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nt)
+    for (int i = 0; i < np; ++i) fit[i] = sse_of(pop.data() + (size_t)i * dim);
+    const double DE_F = 0.6, DE_CR = 0.9;
+    std::vector<double> npop(pop.size()), nfit(np);
+    for (int gen = 0; gen < n_gen; ++gen) {
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nt)
+        for (int i = 0; i < np; ++i) {
+            SmallRng rng = SmallRng::seed_from_u64(splitmix64(seed ^ ((uint64_t)gen << 32) ^ (uint64_t)i));
+            uint64_t idx[3] = {0, 0, 0};
+            for (int slot = 0; slot < 3; ++slot) {
+                for (;;) {
+                    uint64_t cand = rng.gen_range_usize(0, (uint64_t)np);
+                    bool seen = false;
+                    for (int k = 0; k < slot; ++k) seen = seen || idx[k] == cand;
+                    if (cand != (uint64_t)i && !seen) { idx[slot] = cand; break; }
+                }
+            }
+            const double* pa = pop.data() + idx[0] * dim;
+            const double* pb = pop.data() + idx[1] * dim;
+            const double* pc = pop.data() + idx[2] * dim;
+            uint64_t forced = rng.gen_range_usize(0, (uint64_t)dim);
+            double trial[8];
+            for (int d = 0; d < dim; ++d) trial[d] = pop[(size_t)i * dim + d];
+            for (int d = 0; d < dim; ++d)
+                if ((uint64_t)d == forced || rng.gen_f64() < DE_CR)
+                    trial[d] = rust_clamp(pa[d] + DE_F * (pb[d] - pc[d]), lo[d], hi[d]);
+            double tf = sse_of(trial);
+            double* dst = npop.data() + (size_t)i * dim;
+            if (tf < fit[i]) {
+                for (int d = 0; d < dim; ++d) dst[d] = trial[d];
+                nfit[i] = tf;
+            } else {
+                for (int d = 0; d < dim; ++d) dst[d] = pop[(size_t)i * dim + d];
+                nfit[i] = fit[i];
+            }
+        }
+        pop.swap(npop);
+        fit.swap(nfit);
+    }
+    int best = 0;
+    for (int i = 1; i < np; ++i)
+        if (total_key(fit[i]) < total_key(fit[best])) best = i;
+    *de_best_sse = fit[best];
+    *n_pop_used = np;
+    if (pop_out) std::memcpy(pop_out, pop.data(), sizeof(double) * pop.size());
+    if (fit_out) std::memcpy(fit_out, fit.data(), sizeof(double) * np);
+    CalibOut o = calibrate_inner(m, q.data(), n, pop.data() + (size_t)best * dim, prior, reg_weight, jac_mode);
+    std::memcpy(out, &o, sizeof(o));
+}
+
+// The random-number restatement, exposed for its tests.
+uint64_t orc_splitmix64(uint64_t x) { return splitmix64(x); }
+void orc_small_rng_u64(uint64_t seed, int n, uint64_t* out) {
+    SmallRng r = SmallRng::seed_from_u64(seed);
+    for (int i = 0; i < n; ++i) out[i] = r.next_u64();
+}
+void orc_xoshiro_from_state(const uint64_t* state4, int n, uint64_t* out) {
+    SmallRng r;
+    for (int k = 0; k < 4; ++k) r.s[k] = state4[k];
+    for (int i = 0; i < n; ++i) out[i] = r.next_u64();
+}
+void orc_rng_gen_range_f64(uint64_t seed, double lo, double hi, int n, double* out) {
+    SmallRng r = SmallRng::seed_from_u64(seed);
+    for (int i = 0; i < n; ++i) out[i] = r.gen_range_f64(lo, hi);
+}
+void orc_rng_gen_range_usize(uint64_t seed, uint64_t lo, uint64_t hi, int n, uint64_t* out) {
+    SmallRng r = SmallRng::seed_from_u64(seed);
+    for (int i = 0; i < n; ++i) out[i] = r.gen_range_usize(lo, hi);
+}
+void orc_random_guess(int dim, uint64_t seed, double* out) {
+    SmallRng r = SmallRng::seed_from_u64(seed);
+    random_guess(dim, r, out);
 }
 
 // Many independent calibrations (one per surface) over the host cores; the

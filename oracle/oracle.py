@@ -79,6 +79,7 @@ def lib() -> ctypes.CDLL:
         ip = ctypes.POINTER(ctypes.c_int32)
         vp = ctypes.c_void_p
         d, i, i64 = ctypes.c_double, ctypes.c_int, ctypes.c_int64
+        u64, u64p = ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)
         sig = {
             "orc_fast_csqrt": (None, [d, d, dp]),
             "orc_stable_cf": (None, [d, d, d, d, dp, dp]),
@@ -104,6 +105,15 @@ def lib() -> ctypes.CDLL:
             "orc_jacobian": (None, [i, vp, dp, i, dp, dp]),
             "orc_jacobi_eigen": (None, [dp, i, dp, dp]),
             "orc_lm_step": (None, [dp, dp, d, i, dp]),
+            "orc_calibrate_ex": (None, [i, vp, dp, dp, i, dp, dp, d, i, d, vp]),
+            "orc_calibrate_multistart": (None, [i, vp, dp, dp, i, dp, i, u64, i, d, vp, vp, ip, i]),
+            "orc_calibrate_global": (None, [i, vp, dp, dp, i, i, i, u64, dp, d, i, vp, dp, dp, dp, ip, i]),
+            "orc_splitmix64": (u64, [u64]),
+            "orc_small_rng_u64": (None, [u64, i, u64p]),
+            "orc_xoshiro_from_state": (None, [u64p, i, u64p]),
+            "orc_rng_gen_range_f64": (None, [u64, d, d, i, dp]),
+            "orc_rng_gen_range_usize": (None, [u64, u64, u64, i, u64p]),
+            "orc_random_guess": (None, [i, u64, dp]),
             "orc_calib_out_size": (i, []),
             "orc_max_threads": (i, []),
         }
@@ -295,6 +305,104 @@ def calibrate(dim: int, con, iv_market, p0, weight=None, prior=None, reg_weight=
     lib().orc_calibrate(dim, con.ctypes.data, _dptr(iv), None if w is None else _dptr(w), con.size, _dptr(p0),
                         None if pr is None else _dptr(pr), float(reg_weight), out.ctypes.data)
     return out[0]
+
+
+def _quotes(con, iv_market, weight):
+    con = np.ascontiguousarray(con, dtype=CONTRACT_DTYPE)
+    iv = np.ascontiguousarray(iv_market, dtype=np.float64)
+    w = None if weight is None else np.ascontiguousarray(weight, dtype=np.float64)
+    return con, iv, w
+
+
+def calibrate_ex(dim: int, con, iv_market, p0, weight=None, prior=None, reg_weight=0.0, jac_mode: int = 0,
+                 shared_best=float("nan")):
+    """calibrate_inner with every option: Tikhonov prior, the Jacobian variant
+    (0 = the reference's FD/AD, 1 = exact, as the device LM), and a fixed
+    shared best SSE to prune against (NaN = no pruning)."""
+    con, iv, w = _quotes(con, iv_market, weight)
+    p0 = np.ascontiguousarray(p0, dtype=np.float64)
+    pr = None if prior is None else np.ascontiguousarray(prior, dtype=np.float64)
+    out = np.zeros(1, CALIB_OUT_DTYPE)
+    lib().orc_calibrate_ex(dim, con.ctypes.data, _dptr(iv), None if w is None else _dptr(w), con.size, _dptr(p0),
+                           None if pr is None else _dptr(pr), float(reg_weight), int(jac_mode), float(shared_best),
+                           out.ctypes.data)
+    return out[0]
+
+
+def calibrate_multistart(dim: int, con, iv_market, p0, n_restarts: int, seed: int, weight=None, jac_mode: int = 0,
+                         shared_best0=float("inf"), nthreads: int = 0):
+    """calibration.rs:266-314 with the restarts in lockstep.  Returns
+    (best record, all records, n_converged, n_pruned, best index)."""
+    con, iv, w = _quotes(con, iv_market, weight)
+    p0 = np.ascontiguousarray(p0, dtype=np.float64)
+    nr = max(int(n_restarts), 1)
+    best = np.zeros(1, CALIB_OUT_DTYPE)
+    allr = np.zeros(nr, CALIB_OUT_DTYPE)
+    cnt = np.zeros(3, np.int32)
+    lib().orc_calibrate_multistart(dim, con.ctypes.data, _dptr(iv), None if w is None else _dptr(w), con.size,
+                                   _dptr(p0), nr, ctypes.c_uint64(int(seed) & (2**64 - 1)), int(jac_mode),
+                                   float(shared_best0), best.ctypes.data, allr.ctypes.data, _iptr(cnt), int(nthreads))
+    return best[0], allr, int(cnt[0]), int(cnt[1]), int(cnt[2])
+
+
+def calibrate_global(dim: int, con, iv_market, n_pop: int, n_gen: int, seed: int, weight=None, prior=None,
+                     reg_weight=0.0, jac_mode: int = 0, nthreads: int = 0):
+    """calibration.rs:349-427.  Returns (polished record, de_best_sse,
+    final population, final fitness)."""
+    con, iv, w = _quotes(con, iv_market, weight)
+    pr = None if prior is None else np.ascontiguousarray(prior, dtype=np.float64)
+    np_used = max(int(n_pop), 4 * dim)
+    out = np.zeros(1, CALIB_OUT_DTYPE)
+    sse = np.zeros(1)
+    pop = np.zeros((np_used, dim))
+    fit = np.zeros(np_used)
+    npu = np.zeros(1, np.int32)
+    lib().orc_calibrate_global(dim, con.ctypes.data, _dptr(iv), None if w is None else _dptr(w), con.size,
+                               int(n_pop), int(n_gen), ctypes.c_uint64(int(seed) & (2**64 - 1)),
+                               None if pr is None else _dptr(pr), float(reg_weight), int(jac_mode), out.ctypes.data,
+                               _dptr(sse), _dptr(pop), _dptr(fit), _iptr(npu), int(nthreads))
+    assert int(npu[0]) == np_used
+    return out[0], float(sse[0]), pop, fit
+
+
+def _u64p(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
+
+
+def splitmix64(x: int) -> int:
+    return int(lib().orc_splitmix64(ctypes.c_uint64(x & (2**64 - 1))))
+
+
+def small_rng_u64(seed: int, n: int) -> np.ndarray:
+    out = np.zeros(n, np.uint64)
+    lib().orc_small_rng_u64(ctypes.c_uint64(seed & (2**64 - 1)), n, _u64p(out))
+    return out
+
+
+def xoshiro_from_state(state4, n: int) -> np.ndarray:
+    st = np.ascontiguousarray(state4, dtype=np.uint64)
+    out = np.zeros(n, np.uint64)
+    lib().orc_xoshiro_from_state(_u64p(st), n, _u64p(out))
+    return out
+
+
+def rng_gen_range_f64(seed: int, lo: float, hi: float, n: int) -> np.ndarray:
+    out = np.zeros(n)
+    lib().orc_rng_gen_range_f64(ctypes.c_uint64(seed & (2**64 - 1)), lo, hi, n, _dptr(out))
+    return out
+
+
+def rng_gen_range_usize(seed: int, lo: int, hi: int, n: int) -> np.ndarray:
+    out = np.zeros(n, np.uint64)
+    lib().orc_rng_gen_range_usize(ctypes.c_uint64(seed & (2**64 - 1)), lo, hi, n, _u64p(out))
+    return out
+
+
+def random_guess(dim: int, seed: int) -> np.ndarray:
+    """CalibModel::random_guess from SmallRng::seed_from_u64(seed)."""
+    out = np.zeros(dim)
+    lib().orc_random_guess(dim, ctypes.c_uint64(seed & (2**64 - 1)), _dptr(out))
+    return out
 
 
 def calibrate_many(dim: int, con, iv_market, offsets, p0s, nthreads: int = 0) -> np.ndarray:
