@@ -57,6 +57,8 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-calib", action="store_true", help="skip the config-4 calibration section")
+    ap.add_argument("--no-gradient", action="store_true", help="skip the adjoint-gradient section")
+    ap.add_argument("--grad-n", type=int, default=1 << 18, help="contracts in the adjoint-gradient section")
     ap.add_argument("--no-serving", action="store_true", help="skip the config-5 serving section")
     ap.add_argument("--serving-rates", default="100,1000,5000,20000")
     return ap.parse_args()
@@ -229,6 +231,126 @@ def bench_calibration(args) -> dict:
                                "kind": "port", "sample": f"{k} surfaces, reference LM with FD Jacobian, "
                                                          f"one surface per thread, {dt:.1f} s",
                                "rmse_max_abs_diff_vs_gpu": float(np.max(np.abs(ro["rmse"] - r["rmse"][:k])))}
+    out["multistart"] = bench_multistart(args, con, iv, off, p0)
+    out["global"] = bench_global(args, con, iv, off)
+    return out
+
+
+def bench_multistart(args, con, iv, off, p0, n_surf=64, n_restarts=8, seed=12345) -> dict:
+    """calibration.rs:246-314 on the first n_surf config-4 surfaces: every
+    restart of every surface one LM state machine of one device graph, restarts
+    of a surface pruning against their shared best."""
+    import ope_b200 as ope
+
+    o = off[:n_surf + 1]
+    c, v = con[:o[-1]], iv[:o[-1]]
+    ope.calibrate_multistart(ope.MODEL_HESTON, c, v, o, p0[:n_surf], n_restarts, seed)  # builds the graph
+    t0 = time.perf_counter()
+    r = ope.calibrate_multistart(ope.MODEL_HESTON, c, v, o, p0[:n_surf], n_restarts, seed)
+    dt = time.perf_counter() - t0
+    out = {"surfaces": n_surf, "restarts": n_restarts, "value": n_surf / dt, "unit": "surfaces/s", "ms": 1e3 * dt,
+           "pruned_per_surface": float(r["n_pruned"].mean()), "converged_per_surface": float(r["n_converged"].mean()),
+           "best_rmse_median": float(np.median(r["best"]["rmse"]))}
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+
+        t0 = time.perf_counter()
+        best, _, _, _, _ = O.calibrate_multistart(5, con[:off[1]], iv[:off[1]], p0[0], n_restarts, seed)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": 1.0 / dt, "unit": "surfaces/s", "cores": O.max_threads(), "kind": "port",
+                               "sample": f"1 surface, {n_restarts} restarts in lockstep over the host cores, "
+                                         f"reference LM (FD Jacobian), {dt:.1f} s",
+                               "best_rmse_abs_diff_vs_gpu": float(abs(best["rmse"] - r["best"]["rmse"][0]))}
+    return out
+
+
+def bench_global(args, con, iv, off, n_surf=16, n_pop=40, n_gen=60, seed=777) -> dict:
+    """calibration.rs:316-427 (DE/rand/1/bin + LM polish) on the first n_surf
+    config-4 surfaces: each generation prices every member of every surface
+    in one persistent launch; the generation loop is one device graph."""
+    import ope_b200 as ope
+
+    o = off[:n_surf + 1]
+    c, v = con[:o[-1]], iv[:o[-1]]
+    ope.calibrate_global(ope.MODEL_HESTON, c[:o[1]], v[:o[1]], o[:2], n_pop, 1, seed)  # warm
+    t0 = time.perf_counter()
+    r = ope.calibrate_global(ope.MODEL_HESTON, c, v, o, n_pop, n_gen, seed)
+    dt = time.perf_counter() - t0
+    pricings = int(o[-1]) * n_pop * (n_gen + 1)
+    out = {"surfaces": n_surf, "n_pop": n_pop, "n_gen": n_gen, "value": n_surf / dt, "unit": "surfaces/s",
+           "ms": 1e3 * dt, "member_pricings": pricings, "member_pricings_per_s": pricings / dt,
+           "rmse_median": float(np.median(r["best"]["rmse"]))}
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+
+        t0 = time.perf_counter()
+        ro, sse, _, _ = O.calibrate_global(5, con[:off[1]], iv[:off[1]], n_pop, n_gen, seed)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": 1.0 / dt, "unit": "surfaces/s", "cores": O.max_threads(), "kind": "port",
+                               "sample": f"1 surface, population over the host cores, reference LM polish, "
+                                         f"{dt:.1f} s",
+                               "de_best_sse_rel_diff_vs_gpu": float(abs(sse - r["de_best_sse"][0]) / sse)}
+    return out
+
+
+def bench_gradient(args, w, dev, flush, stream, price_kernel_ms) -> dict:
+    """Prices + d price / d(v0, kappa, theta, sigma, rho, lambda, mu_j, sigma_j)
+    by the reverse-mode adjoint kernel (ad.rs:695-731, 882-895) on the first
+    grad_n contracts of the pricing workload, device-resident, L2 flushed,
+    CUDA events; checked against the oracle's forward-mode AD on a sample."""
+    import torch
+
+    import ope_b200 as ope
+
+    n_surf = int(np.searchsorted(w.surf_offsets, min(args.grad_n, w.n), side="right") - 1)
+    n = int(w.surf_offsets[n_surf])
+    d_con = torch.from_numpy(w.contracts[:n].view(np.uint8).copy()).to(dev)
+    d_off = torch.from_numpy(w.surf_offsets[:n_surf + 1].copy()).to(dev)
+    d_par = torch.from_numpy(w.params[:n_surf].copy()).to(dev)
+    d_px = torch.empty(n, dtype=torch.float64, device=dev)
+    d_g = torch.empty((n, 8), dtype=torch.float64, device=dev)
+
+    def step():
+        ope.price_gradient_surfaces_device(ope.MODEL_BATES, d_con, n, d_off, n_surf, d_par, d_px, d_g, tol=w.tol,
+                                           stream=stream.cuda_stream)
+
+    for _ in range(max(args.warmup, 3)):
+        flush.zero_()
+        step()
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        step()
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(b))
+    k_ms = statistics.mean(ms)
+    out = {"workload": f"c3-bates-deepwing first {n} contracts ({n_surf} surfaces)", "n_contracts": n,
+           "params_per_contract": 8, "value": n / (k_ms * 1e-3), "unit": "contracts/s (price + 8-parameter gradient)",
+           "kernel_ms": k_ms, "cost_vs_price": (k_ms / n) / (price_kernel_ms / w.n)}
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+
+        rng = np.random.default_rng(7)
+        pick = np.sort(rng.choice(n, 2000, replace=False))
+        sidx = (np.searchsorted(w.surf_offsets, pick, side="right") - 1).astype(np.int32)
+        t0 = time.perf_counter()
+        price, grad = O.batch_price_gradient(w.contracts[pick], w.params, True, w.tol, surf_idx=sidx)
+        dt = time.perf_counter() - t0
+        g = d_g.cpu().numpy()[pick]
+        # relative error with an absolute floor of 1e-9 S per component (the adjoint tests' bar)
+        lim = 1e-7 * np.abs(grad) + 1e-9 * w.contracts["spot"][pick, None]
+        worst = float((np.abs(g - grad) / lim).max())
+        out["cpu_baseline"] = {"value": pick.size / dt, "unit": out["unit"], "cores": O.max_threads(),
+                               "kind": "port", "sample": f"{pick.size} contracts, forward-mode AD, 8 passes each, "
+                                                         f"{dt:.1f} s"}
+        out["parity"] = {"worst_err_over_bar": worst, "bar": "1e-7 relative + 1e-9 S absolute, per component",
+                         "against": "oracle forward-mode AD (ad.rs:695-731, 882-895)",
+                         "max_abs_price_err_over_spot": float(np.max(np.abs(d_px.cpu().numpy()[pick] - price)
+                                                                     / w.contracts["spot"][pick]))}
     return out
 
 
@@ -414,6 +536,8 @@ def run_ours(args) -> None:
                                 "sample": f"{m} random contracts of the workload in {dt:.1f} s"}
         line["parity"] = {"max_abs_err_over_spot": worst, "bar": 1e-9, "contracts_checked": m,
                           "against": "CPU oracle (the reference restated), same tolerance, same contracts"}
+    if rank == 0 and world == 1 and not args.no_gradient:
+        line["gradient"] = bench_gradient(args, w, dev, flush, stream, kern_avg)
     if rank == 0 and world == 1 and not args.no_calib:
         line["calibration"] = bench_calibration(args)
     if rank == 0 and world == 1 and not args.no_serving:

@@ -163,6 +163,16 @@ int ope_price_surfaces(int32_t model, const ope_contract* contracts, size_t n,
                        const int64_t* surf_offsets, size_t n_surf, const void* params,
                        double* out_prices, const ope_options* opts);
 
+/* ad.rs:736-795 heston_greeks_ad / ad.rs:809-865 bates_greeks_ad, batched
+ * over contracts under one parameter set: price and vega from the exact
+ * d price / d v0 (reverse-mode adjoint kernel; vega = dP/dv0 * 2 sqrt(v0)),
+ * volga from the same derivative at v0 = (sqrt(v0) +- 0.01)^2 (lower leg
+ * floored at 1e-6), delta / gamma (spot +- 1%), theta (T - 1 day, floored at
+ * 1e-6), rho (r +- 1bp) and vanna by the reference's finite differences.
+ * Host or device pointers (OPE_FLAG_DEVICE_PTRS). */
+int ope_batch_greeks_ad(int32_t model, const ope_contract* contracts, size_t n, const void* params,
+                        ope_pricing_result* out, const ope_options* opts);
+
 /* batch.rs:51-56 batch_implied_vol (iv.rs:14-95 per contract): BSM implied
  * volatility of market_prices[i] for contracts[i]; out_ok[i] = 0 where the
  * reference returns None (out_iv[i] is then 0). */

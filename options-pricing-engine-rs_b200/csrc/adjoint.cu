@@ -25,7 +25,7 @@
 // Minimum resident blocks per SM for the adjoint kernel's __launch_bounds__
 // (caps registers per thread at 65536 / (128 * OPE_GRAD_MINB)).
 #ifndef OPE_GRAD_MINB
-#define OPE_GRAD_MINB 5
+#define OPE_GRAD_MINB 7
 #endif
 
 namespace ope {
@@ -58,6 +58,7 @@ __global__ void __launch_bounds__(128, OPE_GRAD_MINB) k_price_grad(const ope_con
                                                     unsigned long long* head) {
     constexpr int DIM = BATES ? 8 : 5;
     extern __shared__ PanelStore smem_panels[];
+    __shared__ double s_norm[4][16];  // per warp: the P1 normaliser's dLog CF(-i)/dp (complex, DIM <= 8)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     PanelStore& L = smem_panels[warp];
     const LaneRule R = lane_rule(lane);
@@ -91,23 +92,39 @@ __global__ void __launch_bounds__(128, OPE_GRAD_MINB) k_price_grad(const ope_con
         const double I = gk_integrate_warp<BATES>(C, tol, L, lane, R, &nb);
         const int len = nb + 1;
 
-        // derivative integral over the final panel set
+        // derivative integral over the final panel set; for P1 one extra work
+        // item evaluates the normaliser's dLog CF(-i)/dp (u = 0), so that the
+        // kernel holds ONE inlined copy of exponent_and_grad
         const GradParams G = make_grad_params(pl, BATES);
         double acc[DIM];
 #pragma unroll
         for (int k = 0; k < DIM; ++k) acc[k] = 0.0;
         double sw_re = 0.0, sw_im = 0.0;
         const int total = 15 * len;
-        for (int base = 0; base < total; base += 32) {
+        const int items = total + (which == 0 ? 1 : 0);
+        for (int base = 0; base < items; base += 32) {
             const int idx = base + lane;
             const int pi = idx / 15, j = idx - 15 * (idx / 15);
             const double xj = __shfl_sync(0xffffffffu, R.x, j & 15);
             const double wj = __shfl_sync(0xffffffffu, R.wk, j & 15);
-            if (idx < total) {
-                const double a = L.a[pi], b = L.b[pi];
-                const double cc = 0.5 * (a + b), h = 0.5 * (b - a);
-                const double tn = __dadd_rn(cc, __dmul_rn(h, xj));
-                node_grad<BATES>(C, G, tn, h * wj, acc, sw_re, sw_im);
+            if (idx < items) {
+                const bool normaliser = idx == total;
+                double tn = 0.0, hw = 0.0, u = 0.0;
+                if (!normaliser) {
+                    const double a = L.a[pi], b = L.b[pi];
+                    const double cc = 0.5 * (a + b), h = 0.5 * (b - a);
+                    tn = __dadd_rn(cc, __dmul_rn(h, xj));
+                    hw = h * wj;
+                    u = (1.0 - tn) / tn;
+                }
+                C2 dz[8];
+                const C2 Z = exponent_and_grad<BATES>(C, G, u, dz);
+                if (normaliser) {
+#pragma unroll
+                    for (int k = 0; k < DIM; ++k) { s_norm[warp][2 * k] = dz[k].re; s_norm[warp][2 * k + 1] = dz[k].im; }
+                } else {
+                    node_accumulate<BATES>(Z, dz, tn, u, hw, acc, sw_re, sw_im);
+                }
             }
         }
 #pragma unroll
@@ -117,10 +134,11 @@ __global__ void __launch_bounds__(128, OPE_GRAD_MINB) k_price_grad(const ope_con
         if (which == 0) {
             // -d Log CF(-i)/dp, constant over the integral (zero up to rounding for a
             // regular normaliser; ad.rs:705-706 carries it through the Dual division)
-            C2 dlm[8];
-            exponent_and_grad<BATES>(C, G, 0.0, dlm);
+            __syncwarp();
 #pragma unroll
-            for (int k = 0; k < DIM; ++k) acc[k] -= (dlm[k] * c2(sw_re, sw_im)).im;
+            for (int k = 0; k < DIM; ++k)
+                acc[k] -= (c2(s_norm[warp][2 * k], s_norm[warp][2 * k + 1]) * c2(sw_re, sw_im)).im;
+            __syncwarp();
         }
         if (lane == 0) {
             integ[2 * c + which] = I;

@@ -147,7 +147,7 @@ int batch_price(int32_t model, const ope_contract* contracts, size_t n, const vo
 }
 
 int batch_greeks(int32_t model, const ope_contract* contracts, size_t n, const void* params,
-                 ope_pricing_result* out, const ope_options* opts) {
+                 ope_pricing_result* out, const ope_options* opts, bool ad = false) {
     OPE_TRY(check_model(model));
     double tol;
     OPE_TRY(resolve_tol(opts, &tol));
@@ -155,16 +155,20 @@ int batch_greeks(int32_t model, const ope_contract* contracts, size_t n, const v
     if (!contracts || !params || !out) return set_error(OPE_ERR_INVALID_ARG, "NULL array argument");
     OPE_TRY(ensure_device());
     const int stride = param_stride(model);
+    const size_t g_bytes = ad ? greeks_ad_workspace_bytes(n, stride) : greeks_workspace_bytes(n);
+    auto launch = [&](const ope_contract* con, const double* par, ope_pricing_result* o, void* gws, cudaStream_t st) {
+        return ad ? launch_greeks_ad(model, con, n, par, tol, o, gws, st) : launch_greeks(model, con, n, par, tol, o, gws, st);
+    };
     if (device_ptrs(opts)) {
         void* ws;
-        OPE_TRY(ensure_workspace(greeks_workspace_bytes(n), &ws));
-        return launch_greeks(model, contracts, n, static_cast<const double*>(params), tol, out, ws, user_stream(opts));
+        OPE_TRY(ensure_workspace(g_bytes, &ws));
+        return launch(contracts, static_cast<const double*>(params), out, ws, user_stream(opts));
     }
     ThreadCtx& c = tctx();
     const size_t b_con = align_up(n * sizeof(ope_contract), 256), b_par = 256,
                  b_out = align_up(n * sizeof(ope_pricing_result), 256);
     void* ws;
-    OPE_TRY(ensure_workspace(b_con + b_par + b_out + greeks_workspace_bytes(n), &ws));
+    OPE_TRY(ensure_workspace(b_con + b_par + b_out + g_bytes, &ws));
     char* p = static_cast<char*>(ws);
     ope_contract* d_con = reinterpret_cast<ope_contract*>(p);
     double* d_par = reinterpret_cast<double*>(p + b_con);
@@ -172,7 +176,7 @@ int batch_greeks(int32_t model, const ope_contract* contracts, size_t n, const v
     void* gws = p + b_con + b_par + b_out;
     OPE_CHECK(cudaMemcpyAsync(d_con, contracts, n * sizeof(ope_contract), cudaMemcpyHostToDevice, c.stream));
     OPE_CHECK(cudaMemcpyAsync(d_par, params, stride * sizeof(double), cudaMemcpyHostToDevice, c.stream));
-    OPE_TRY(launch_greeks(model, d_con, n, d_par, tol, d_out, gws, c.stream));
+    OPE_TRY(launch(d_con, d_par, d_out, gws, c.stream));
     OPE_CHECK(cudaMemcpyAsync(out, d_out, n * sizeof(ope_pricing_result), cudaMemcpyDeviceToHost, c.stream));
     OPE_CHECK(cudaStreamSynchronize(c.stream));
     return OPE_OK;
@@ -241,6 +245,11 @@ int ope_batch_price_ex(int32_t model, const ope_contract* contracts, size_t n, c
 int ope_batch_greeks_ex(int32_t model, const ope_contract* contracts, size_t n, const void* params,
                         ope_pricing_result* out, const ope_options* opts) {
     return batch_greeks(model, contracts, n, params, out, opts);
+}
+
+int ope_batch_greeks_ad(int32_t model, const ope_contract* contracts, size_t n, const void* params,
+                        ope_pricing_result* out, const ope_options* opts) {
+    return batch_greeks(model, contracts, n, params, out, opts, true);
 }
 
 int ope_batch_implied_vol(const ope_contract* contracts, size_t n, const double* market_prices, double* out_iv,

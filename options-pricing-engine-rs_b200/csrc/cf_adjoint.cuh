@@ -135,17 +135,15 @@ __device__ __forceinline__ C2 exponent_and_grad(const CfConsts& C, const GradPar
     return Z;
 }
 
-// One node of the derivative integral: returns g(t) and adds hw * dg/dp into
-// acc[0..dim); adds hw * W/(u t^2) into sw (for the P1 normaliser term).
-// A node whose value or derivative is not finite contributes zero, as in
+// One node of the derivative integral from its exponent Z and dZ/dp (from
+// exponent_and_grad at u = (1 - tn)/tn): adds hw * dg/dp into acc[0..dim)
+// and hw * W/(u t^2) into sw (for the P1 normaliser term).  A node whose
+// value or derivative is not finite contributes zero, as in
 // gk_integrate_dual (ad.rs:679-682).
 template <bool BATES>
-__device__ __forceinline__ double node_grad(const CfConsts& C, const GradParams& P, double tn, double hw, double* acc,
-                                            double& sw_re, double& sw_im) {
+__device__ __forceinline__ void node_accumulate(const C2& Z, const C2* dz, double tn, double u, double hw,
+                                                double* acc, double& sw_re, double& sw_im) {
     constexpr int DIM = BATES ? 8 : 5;
-    const double u = (1.0 - tn) / tn;
-    C2 dz[8];
-    const C2 Z = exponent_and_grad<BATES>(C, P, u, dz);
     double sn, cs;
     sincos(Z.im, &sn, &cs);
     const double ez = exp(Z.re);
@@ -165,7 +163,6 @@ __device__ __forceinline__ double node_grad(const CfConsts& C, const GradParams&
         sw_re += hw * Wf.re;
         sw_im += hw * Wf.im;
     }
-    return ok ? v : 0.0;
 }
 
 }  // namespace ope

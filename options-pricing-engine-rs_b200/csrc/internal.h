@@ -122,6 +122,11 @@ int selftest_math(uint64_t* ulp_rcp, uint64_t* ulp_sqrt);
 size_t greeks_workspace_bytes(size_t n);
 int launch_greeks(int model, const ope_contract* con, size_t n, const double* params, double tol,
                   ope_pricing_result* out, void* ws, cudaStream_t st);
+// AD Greeks (ad.rs:736-795, 809-865) for n contracts under one parameter set;
+// `ws` must hold greeks_ad_workspace_bytes(n, dim) bytes.
+size_t greeks_ad_workspace_bytes(size_t n, int dim);
+int launch_greeks_ad(int model, const ope_contract* con, size_t n, const double* params, double tol,
+                     ope_pricing_result* out, void* ws, cudaStream_t st);
 
 inline int param_stride(int model) { return model == OPE_MODEL_BATES ? 8 : 5; }
 

@@ -173,36 +173,159 @@ inline std::vector<std::optional<double>> batch_implied_vol(const std::vector<Op
     return out;
 }
 
+// ad.rs:736-795
+inline PricingResult heston_greeks_ad(double spot, double strike, double expiry, double rate, double div_yield,
+                                      const HestonParams& params, OptionType opt_type) {
+    const ope_contract c{spot, strike, expiry, rate, div_yield, 0.0, static_cast<int32_t>(opt_type), 0};
+    const double p[5] = {params.v0, params.kappa, params.theta, params.sigma, params.rho};
+    PricingResult r;
+    check(ope_batch_greeks_ad(OPE_MODEL_HESTON, &c, 1, p, &r, nullptr));
+    return r;
+}
+
+// ad.rs:809-865
+inline PricingResult bates_greeks_ad(double spot, double strike, double expiry, double rate, double div_yield,
+                                     const HestonParams& heston, double lambda, double mu_j, double sigma_j,
+                                     OptionType opt_type) {
+    const ope_contract c{spot, strike, expiry, rate, div_yield, 0.0, static_cast<int32_t>(opt_type), 0};
+    const double p[8] = {heston.v0, heston.kappa, heston.theta, heston.sigma, heston.rho, lambda, mu_j, sigma_j};
+    PricingResult r;
+    check(ope_batch_greeks_ad(OPE_MODEL_BATES, &c, 1, p, &r, nullptr));
+    return r;
+}
+
+struct MultistartResult {  // calibration.rs:70-76
+    CalibResult best;
+    size_t n_restarts, n_converged, n_pruned;
+};
+
+struct GlobalCalibResult {  // calibration.rs:296-300
+    CalibResult best;
+    double de_best_sse;
+    size_t de_generations;
+};
+
 namespace detail {
-inline CalibResult calibrate(int model, const std::vector<CalibInput>& quotes, const std::vector<double>& p0) {
-    if (quotes.empty()) throw Error(OPE_ERR_INVALID_ARG, "nothing to calibrate");  // calibration.rs:438
+struct Quotes {
     std::vector<ope_contract> c;
     std::vector<double> iv, w;
-    for (const auto& q : quotes) {
-        c.push_back(to_c(*q.contract));
-        iv.push_back(q.iv_market);
-        w.push_back(q.weight);
+    int64_t off[2];
+    explicit Quotes(const std::vector<CalibInput>& quotes) {
+        if (quotes.empty()) throw Error(OPE_ERR_INVALID_ARG, "nothing to calibrate");  // calibration.rs:438
+        for (const auto& q : quotes) {
+            c.push_back(to_c(*q.contract));
+            iv.push_back(q.iv_market);
+            w.push_back(q.weight);
+        }
+        off[0] = 0;
+        off[1] = (int64_t)c.size();
     }
-    const int64_t off[2] = {0, (int64_t)c.size()};
-    ope_calib_result r;
-    check(ope_calibrate_surfaces(model, c.data(), iv.data(), w.data(), c.size(), off, 1, p0.data(), &r, nullptr));
-    const size_t dim = p0.size();
+};
+inline CalibResult from_c(const ope_calib_result& r, size_t dim) {
     return CalibResult{std::vector<double>(r.params, r.params + dim), r.rmse, r.max_err, r.iters,
                        r.converged != 0, r.early_stopped != 0, r.condition_number,
                        std::vector<double>(r.weakest_direction, r.weakest_direction + dim)};
+}
+inline std::vector<double> vec(const HestonParams& p) { return {p.v0, p.kappa, p.theta, p.sigma, p.rho}; }
+inline std::vector<double> vec(const BatesParams& p) {
+    return {p.heston.v0, p.heston.kappa, p.heston.theta, p.heston.sigma, p.heston.rho, p.lambda, p.mu_j, p.sigma_j};
+}
+inline CalibResult calibrate(int model, const std::vector<CalibInput>& quotes, const std::vector<double>& p0) {
+    Quotes q(quotes);
+    ope_calib_result r;
+    check(ope_calibrate_surfaces(model, q.c.data(), q.iv.data(), q.w.data(), q.c.size(), q.off, 1, p0.data(), &r,
+                                 nullptr));
+    return from_c(r, p0.size());
+}
+inline CalibResult calibrate_reg(int model, const std::vector<CalibInput>& quotes, const std::vector<double>& p0,
+                                 const std::vector<double>& prior, double reg_weight) {
+    Quotes q(quotes);
+    ope_calib_result r;
+    check(ope_calibrate_surfaces_reg(model, q.c.data(), q.iv.data(), q.w.data(), q.c.size(), q.off, 1, p0.data(),
+                                     prior.data(), &reg_weight, &r, nullptr));
+    return from_c(r, p0.size());
+}
+inline MultistartResult multistart(int model, const std::vector<CalibInput>& quotes, const std::vector<double>& p0,
+                                   size_t n_restarts, uint64_t seed) {
+    Quotes q(quotes);
+    ope_multistart_result r;
+    check(ope_calibrate_multistart(model, q.c.data(), q.iv.data(), q.w.data(), q.c.size(), q.off, 1, p0.data(),
+                                   (int32_t)n_restarts, seed, nullptr, &r, nullptr, nullptr));
+    return MultistartResult{from_c(r.best, p0.size()), (size_t)r.n_restarts, (size_t)r.n_converged,
+                            (size_t)r.n_pruned};
+}
+inline GlobalCalibResult global(int model, const std::vector<CalibInput>& quotes, size_t n_pop, size_t n_gen,
+                                uint64_t seed, const std::vector<double>* prior, double reg_weight) {
+    Quotes q(quotes);
+    ope_global_result r;
+    check(ope_calibrate_global(model, q.c.data(), q.iv.data(), q.w.data(), q.c.size(), q.off, 1, (int32_t)n_pop,
+                               (int32_t)n_gen, seed, prior ? prior->data() : nullptr, prior ? &reg_weight : nullptr,
+                               &r, nullptr));
+    return GlobalCalibResult{from_c(r.best, model == OPE_MODEL_BATES ? 8 : 5), r.de_best_sse,
+                             (size_t)r.de_generations};
 }
 }  // namespace detail
 
 // calibration.rs:204-206
 inline CalibResult calibrate_heston(const std::vector<CalibInput>& quotes, const HestonParams& p0) {
-    return detail::calibrate(OPE_MODEL_HESTON, quotes, {p0.v0, p0.kappa, p0.theta, p0.sigma, p0.rho});
+    return detail::calibrate(OPE_MODEL_HESTON, quotes, detail::vec(p0));
 }
 
 // calibration.rs:208-210
 inline CalibResult calibrate_bates(const std::vector<CalibInput>& quotes, const BatesParams& p0) {
-    return detail::calibrate(OPE_MODEL_BATES, quotes,
-                             {p0.heston.v0, p0.heston.kappa, p0.heston.theta, p0.heston.sigma, p0.heston.rho,
-                              p0.lambda, p0.mu_j, p0.sigma_j});
+    return detail::calibrate(OPE_MODEL_BATES, quotes, detail::vec(p0));
+}
+
+// calibration.rs:220-224
+inline CalibResult calibrate_heston_regularized(const std::vector<CalibInput>& quotes, const HestonParams& p0,
+                                                const HestonParams& prior, double reg_weight) {
+    return detail::calibrate_reg(OPE_MODEL_HESTON, quotes, detail::vec(p0), detail::vec(prior), reg_weight);
+}
+
+// calibration.rs:226-230
+inline CalibResult calibrate_bates_regularized(const std::vector<CalibInput>& quotes, const BatesParams& p0,
+                                               const BatesParams& prior, double reg_weight) {
+    return detail::calibrate_reg(OPE_MODEL_BATES, quotes, detail::vec(p0), detail::vec(prior), reg_weight);
+}
+
+// calibration.rs:246-250
+inline MultistartResult calibrate_heston_multistart(const std::vector<CalibInput>& quotes, const HestonParams& p0,
+                                                    size_t n_restarts, uint64_t seed) {
+    return detail::multistart(OPE_MODEL_HESTON, quotes, detail::vec(p0), n_restarts, seed);
+}
+
+// calibration.rs:252-256
+inline MultistartResult calibrate_bates_multistart(const std::vector<CalibInput>& quotes, const BatesParams& p0,
+                                                   size_t n_restarts, uint64_t seed) {
+    return detail::multistart(OPE_MODEL_BATES, quotes, detail::vec(p0), n_restarts, seed);
+}
+
+// calibration.rs:316-320
+inline GlobalCalibResult calibrate_heston_global(const std::vector<CalibInput>& quotes, size_t n_pop, size_t n_gen,
+                                                 uint64_t seed) {
+    return detail::global(OPE_MODEL_HESTON, quotes, n_pop, n_gen, seed, nullptr, 0.0);
+}
+
+// calibration.rs:322-326
+inline GlobalCalibResult calibrate_bates_global(const std::vector<CalibInput>& quotes, size_t n_pop, size_t n_gen,
+                                                uint64_t seed) {
+    return detail::global(OPE_MODEL_BATES, quotes, n_pop, n_gen, seed, nullptr, 0.0);
+}
+
+// calibration.rs:335-340
+inline GlobalCalibResult calibrate_heston_global_regularized(const std::vector<CalibInput>& quotes, size_t n_pop,
+                                                             size_t n_gen, uint64_t seed, const HestonParams& prior,
+                                                             double reg_weight) {
+    const auto pr = detail::vec(prior);
+    return detail::global(OPE_MODEL_HESTON, quotes, n_pop, n_gen, seed, &pr, reg_weight);
+}
+
+// calibration.rs:342-347
+inline GlobalCalibResult calibrate_bates_global_regularized(const std::vector<CalibInput>& quotes, size_t n_pop,
+                                                            size_t n_gen, uint64_t seed, const BatesParams& prior,
+                                                            double reg_weight) {
+    const auto pr = detail::vec(prior);
+    return detail::global(OPE_MODEL_BATES, quotes, n_pop, n_gen, seed, &pr, reg_weight);
 }
 
 }  // namespace ope

@@ -67,6 +67,7 @@ _sig("ope_batch_heston_greeks", ctypes.c_int, [_vp, _sz, _vp, _vp])
 _sig("ope_batch_bates_greeks", ctypes.c_int, [_vp, _sz, _vp, _vp])
 _sig("ope_batch_price_ex", ctypes.c_int, [_i32, _vp, _sz, _vp, _vp, ctypes.POINTER(Options)])
 _sig("ope_batch_greeks_ex", ctypes.c_int, [_i32, _vp, _sz, _vp, _vp, ctypes.POINTER(Options)])
+_sig("ope_batch_greeks_ad", ctypes.c_int, [_i32, _vp, _sz, _vp, _vp, ctypes.POINTER(Options)])
 _sig("ope_price_surfaces", ctypes.c_int, [_i32, _vp, _sz, _vp, _sz, _vp, _vp, ctypes.POINTER(Options)])
 
 _sig("ope_price_surfaces_stats", ctypes.c_int,

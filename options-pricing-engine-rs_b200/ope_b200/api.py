@@ -172,6 +172,35 @@ def batch_bates_greeks(contracts, params, tol=REF_TOL) -> np.ndarray:
     return _batch_greeks(MODEL_BATES, contracts, params, tol)
 
 
+def batch_greeks_ad(model: int, contracts, params, tol=REF_TOL) -> np.ndarray:
+    """ad.rs:736-795 / 809-865 for many contracts under one parameter set: vega and
+    volga from the exact d price / d v0 (adjoint kernel), the rest by the
+    reference's finite differences.  Structured array of PricingResult."""
+    con = contracts_array(contracts)
+    p = _params_array(params, model)
+    out = np.zeros(con.size, dtype=RESULT_DTYPE)
+    if con.size == 0:
+        return out
+    o = _opts(tol)
+    check(load().ope_batch_greeks_ad(model, con.ctypes.data, con.size, p.ctypes.data, out.ctypes.data,
+                                     ctypes.byref(o)))
+    return out
+
+
+def heston_greeks_ad(spot, strike, expiry, rate, div_yield, params, opt_type=OptionType.Call, tol=REF_TOL):
+    """ad.rs:736-795 (one contract): a PricingResult record."""
+    c = [OptionContract(spot, strike, expiry, rate, div_yield, 0.0, OptionType(opt_type))]
+    return batch_greeks_ad(MODEL_HESTON, c, params, tol)[0]
+
+
+def bates_greeks_ad(spot, strike, expiry, rate, div_yield, heston, lam, mu_j, sigma_j, opt_type=OptionType.Call,
+                    tol=REF_TOL):
+    """ad.rs:809-865 (one contract, the reference's argument order): a PricingResult record."""
+    c = [OptionContract(spot, strike, expiry, rate, div_yield, 0.0, OptionType(opt_type))]
+    hp = _params_array(heston, MODEL_HESTON)
+    return batch_greeks_ad(MODEL_BATES, c, np.concatenate([hp, [lam, mu_j, sigma_j]]), tol)[0]
+
+
 def price_surfaces(model: int, contracts, surf_offsets, params, tol=REF_TOL, out=None,
                    bisections=None) -> np.ndarray:
     """Many surfaces (one parameter set each) in ONE persistent launch.
@@ -459,6 +488,15 @@ def price_surfaces_device(model: int, d_contracts, n: int, d_offsets, n_surf: in
                                     ctypes.byref(o)))
 
 
+def price_gradient_surfaces_device(model: int, d_contracts, n: int, d_offsets, n_surf: int, d_params, d_prices,
+                                   d_grad, tol=REF_TOL, stream: int | None = None) -> None:
+    """Stream-ordered adjoint launch (prices + n x dim gradient) over device buffers."""
+    ptr = lambda t: t if isinstance(t, int) else t.data_ptr()  # noqa: E731
+    o = _opts(tol, _lib.FLAG_DEVICE_PTRS, _torch_stream_ptr() if stream is None else stream)
+    check(load().ope_price_gradient_surfaces(model, ptr(d_contracts), n, ptr(d_offsets), n_surf, ptr(d_params),
+                                             ptr(d_prices), ptr(d_grad), ctypes.byref(o)))
+
+
 def batch_price_device(model: int, d_contracts, n: int, d_params, d_out, tol=REF_TOL,
                        stream: int | None = None) -> None:
     """Stream-ordered plain (single parameter set) launch over device buffers."""
@@ -482,6 +520,7 @@ __all__ = [
     "heston_price", "bates_price", "batch_heston", "batch_bates", "batch_heston_greeks", "batch_bates_greeks",
     "price_surfaces", "price_surfaces_device", "batch_price_device", "contracts_array", "REF_TOL",
     "MODEL_HESTON", "MODEL_BATES", "RESULT_DTYPE", "kernel_launch_count", "device_info", "measure_fp64_peak", "price_gradient_surfaces",
+    "price_gradient_surfaces_device", "batch_greeks_ad", "heston_greeks_ad", "bates_greeks_ad",
     "CALIB_RESULT_DTYPE", "batch_implied_vol", "calibrate_surfaces", "calibrate_heston", "calibrate_bates", "calib_jacobian",
     "MULTISTART_RESULT_DTYPE", "GLOBAL_RESULT_DTYPE", "calibrate_surfaces_reg", "calibrate_multistart",
     "calibrate_global", "calibrate_heston_regularized", "calibrate_bates_regularized", "calibrate_heston_multistart",

@@ -1,7 +1,7 @@
 // The reference crate's own unit tests for the CF pricing path, written
 // against the C++ mirror (options-pricing-engine-rs_b200/host/ope.hpp) and so
 // run on the GPU: heston.rs:309-427, bates.rs:98-173, batch.rs:246-319,
-// calibration.rs:1020-1071.  Same inputs, same assertions, same tolerances.
+// calibration.rs:870-1071, 1073-1131, 1216-1234.  Same inputs, same assertions, same tolerances.
 // Exit status 0 when every test passes.
 #include <cmath>
 #include <cstdio>
@@ -244,6 +244,74 @@ int main() {
         EXPECT(res.converged, "did not converge after %d iters", res.iters);
         EXPECT(res.rmse < 0.01, "rmse=%g", res.rmse);
         EXPECT(std::fabs(res.params[0] - 0.04) < 0.01, "v0 off");
+    });
+    auto quotes_of = [](const std::vector<OptionContract>& store, const std::vector<double>& iv) {
+        std::vector<CalibInput> q;
+        for (size_t i = 0; i < store.size(); ++i) q.push_back(CalibInput{&store[i], iv[i], 1.0});
+        return q;
+    };
+    const BatesParams truth_b{{0.04, 2.0, 0.04, 0.3, -0.5}, 0.5, -0.1, 0.15};
+    std::vector<OptionContract> store_h, store_b;
+    const auto iv_h = make_quotes(false, truth_b, store_h);
+    const auto iv_b = make_quotes(true, truth_b, store_b);
+    run("calibration::regularization_recovers_plausible_params_in_the_degenerate_case", [&] {
+        const BatesParams prior{{0.035, 1.8, 0.04, 0.35, -0.45}, 0.4, -0.08, 0.12};
+        const auto reg = calibrate_bates_global_regularized(quotes_of(store_b, iv_b), 60, 80, 999, prior, 1e-3);
+        EXPECT(reg.best.rmse < 0.005, "rmse=%g", reg.best.rmse);
+        EXPECT(std::isfinite(reg.best.condition_number) && reg.best.condition_number < 1e9, "cond=%g",
+               reg.best.condition_number);
+        const auto& p = reg.best.params;
+        EXPECT(std::fabs(p[0] - 0.04) < 0.01, "v0=%g", p[0]);
+        EXPECT(std::fabs(p[1] - 2.0) < 0.5, "kappa=%g", p[1]);
+        EXPECT(std::fabs(p[5] - 0.5) < 0.15, "lambda=%g", p[5]);
+        EXPECT(std::fabs(p[6] + 0.1) < 0.05, "mu_j=%g", p[6]);
+        EXPECT(std::fabs(p[7] - 0.15) < 0.05, "sigma_j=%g", p[7]);
+    });
+    run("calibration::regularization_does_not_hurt_a_well_identified_case", [&] {
+        const auto q = quotes_of(store_h, iv_h);
+        const HestonParams p0{0.05, 1.5, 0.05, 0.4, -0.3};
+        const auto unreg = calibrate_heston(q, p0);
+        const auto reg = calibrate_heston_regularized(q, p0, HestonParams{0.045, 1.8, 0.045, 0.32, -0.45}, 1e-3);
+        EXPECT(reg.rmse < 0.002, "rmse=%g", reg.rmse);
+        EXPECT(std::fabs(reg.params[0] - unreg.params[0]) < 0.005, "v0 drifted");
+    });
+    run("calibration::condition_number_flags_the_degenerate_bates_case", [&] {
+        const auto h = calibrate_heston(quotes_of(store_h, iv_h), HestonParams{0.05, 1.5, 0.05, 0.4, -0.3});
+        EXPECT(std::isfinite(h.condition_number) && h.condition_number < 1e9, "cond=%g", h.condition_number);
+        const auto qb = quotes_of(store_b, iv_b);
+        const auto good = calibrate_bates(qb, BatesParams{{0.05, 1.5, 0.05, 0.4, -0.3}, 0.3, -0.05, 0.1});
+        EXPECT(std::isfinite(good.condition_number), "good p0 degenerate");
+        const auto de = calibrate_bates_global(qb, 60, 80, 999);
+        EXPECT(de.best.condition_number > 1e10 || !std::isfinite(de.best.condition_number), "cond=%g",
+               de.best.condition_number);
+        EXPECT(de.best.condition_number > 100.0 * good.condition_number, "de=%g good=%g", de.best.condition_number,
+               good.condition_number);
+    });
+    run("calibration::de_global_recovers_heston_params_without_any_initial_guess", [&] {
+        const auto res = calibrate_heston_global(quotes_of(store_h, iv_h), 40, 60, 777);
+        const auto& p = res.best.params;
+        EXPECT(res.best.rmse < 0.01, "rmse=%g", res.best.rmse);
+        EXPECT(std::fabs(p[0] - 0.04) < 0.01, "v0 off: %g", p[0]);
+        EXPECT(std::fabs(p[4] + 0.5) < 0.1, "rho off: %g", p[4]);
+        EXPECT(2.0 * p[1] * p[2] > p[3] * p[3], "Feller");
+        const double de_rmse = std::sqrt(res.de_best_sse / (double)iv_h.size());
+        EXPECT(res.best.rmse <= de_rmse + 1e-9, "polished=%g de_raw=%g", res.best.rmse, de_rmse);
+    });
+    run("calibration::de_global_bates_finds_an_excellent_fit_not_necessarily_the_true_params", [&] {
+        const auto res = calibrate_bates_global(quotes_of(store_b, iv_b), 60, 80, 999);
+        const auto& p = res.best.params;
+        EXPECT(res.best.rmse < 0.005, "rmse=%g", res.best.rmse);
+        EXPECT(2.0 * p[1] * p[2] > p[3] * p[3], "Feller");
+        EXPECT(p[0] > 0.0 && p[5] >= 0.0, "sanity bounds");
+    });
+    run("calibration::multistart_beats_bad_single_start", [&] {
+        const auto q = quotes_of(store_h, iv_h);
+        const HestonParams bad{0.25, 6.0, 0.3, 0.15, 0.6};
+        const auto single = calibrate_heston(q, bad);
+        const auto multi = calibrate_heston_multistart(q, bad, 8, 12345);
+        EXPECT(multi.n_converged >= 1, "no restart converged at all");
+        EXPECT(multi.best.rmse <= single.rmse + 1e-9, "multistart=%g single=%g", multi.best.rmse, single.rmse);
+        EXPECT(multi.best.rmse < 0.01, "rmse=%g", multi.best.rmse);
     });
     // ------------------------------------------------------------- error path
     run("errors::invalid_argument_throws", [] {
