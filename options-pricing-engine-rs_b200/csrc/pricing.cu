@@ -23,7 +23,7 @@
 #define OPE_KERNEL_WARPS 4
 #endif
 #ifndef OPE_KERNEL_MINB
-#define OPE_KERNEL_MINB 6
+#define OPE_KERNEL_MINB 7
 #endif
 
 namespace ope {
