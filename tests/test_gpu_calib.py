@@ -98,3 +98,26 @@ def test_graph_rerun_is_deterministic(ope, oracle):
     alone = ope.calibrate_surfaces(ope.MODEL_HESTON, con[off[s]:off[s + 1]], iv[off[s]:off[s + 1]],
                                    [0, off[s + 1] - off[s]], p0[s:s + 1])
     assert alone[0].tobytes() == a[s].tobytes()
+
+
+def test_bates_jacobian_jump_columns_match_pure_fd(ope, oracle):  # calibration.rs:1133-1171
+    """The device Jacobian's lambda / mu_j / sigma_j columns against central
+    differences (h = 1e-4) of the IV residual computed independently, with the
+    device pricer and the device IV solver, at the reference's 2 % bar."""
+    p = np.array([0.045, 1.8, 0.045, 0.35, -0.55, 0.4, -0.08, 0.12])
+    con, iv = _make_quotes(oracle, p, bates=True)
+    J, _ = ope.calib_jacobian(ope.MODEL_BATES, con, iv, [0, iv.size], p[None, :])
+
+    def resid(q):
+        px = ope.batch_bates(con, q)
+        ivm, ok = ope.batch_implied_vol(con, px)
+        return np.where(ok, ivm - iv, 0.0)
+
+    h = 1e-4
+    for col in (5, 6, 7):
+        up, dn = p.copy(), p.copy()
+        up[col] += h
+        dn[col] -= h
+        fd = (resid(up) - resid(dn)) / (2.0 * h)
+        err = np.abs(J[:, col] - fd) / np.maximum(np.abs(fd), 1e-6)
+        assert np.all(err < 0.02), (col, float(err.max()))
