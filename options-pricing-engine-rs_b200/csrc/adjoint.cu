@@ -1,19 +1,25 @@
-// Price + reverse-mode gradient kernel: d price / d(v0, kappa, theta, sigma,
-// rho[, lambda, mu_j, sigma_j]) for every contract of many surfaces.
+// Price + reverse-mode gradient: d price / d(v0, kappa, theta, sigma, rho[,
+// lambda, mu_j, sigma_j]) for every contract of many surfaces.
 //
 // Reference: ad.rs:695-731 (forward_pass: derivative integrated by Leibniz
 // over the primal's adaptive panel set, error control on the primal only),
 // ad.rs:736-745 / 821-825 (the five Heston-parameter passes) and ad.rs:882-895
-// (the three jump-parameter passes).  One unit = one integral, one warp:
-//   1. the primal greedy GK15 integration (identical to the pricing kernel),
-//      leaving the final live-panel list in shared memory;
-//   2. the derivative integral over those panels: the 15 * len nodes are
-//      spread over the 32 lanes, each lane recomputes the CF at its node and
-//      runs the backward pass (cf_adjoint.cuh), accumulating all parameter
-//      derivatives at once; a warp reduction finishes the sums.
-// The price combination is heston.rs:95-98 and the derivative combination is
-// ad.rs:713-730: d price = S e^{-qT} dI1/pi - K e^{-rT} dI2/pi for calls and
-// puts alike (parity terms do not depend on the model parameters).
+// (the three jump-parameter passes).  Three launches:
+//   1. the pricing kernel itself (pricing.cu), which also stores every
+//      integral's final live-panel list (prices are therefore bit-identical
+//      to a plain pricing call);
+//   2. the backward pass, one warp per integral from a work queue: the
+//      15 * len nodes of the stored panels are spread over the 32 lanes, each
+//      lane recomputes the CF at its node and runs the backward pass
+//      (cf_adjoint.cuh), accumulating all parameter derivatives at once; for
+//      P1 one extra work item evaluates the normaliser's dLog CF(-i)/dp; a
+//      warp reduction finishes the sums;
+//   3. a per-contract combine: ad.rs:713-730, d price = S e^{-qT} dI1/pi -
+//      K e^{-rT} dI2/pi for calls and puts alike (parity terms do not depend
+//      on the model parameters).
+// Splitting the primal from the backward pass keeps each kernel's code small
+// (the fused form stalled on instruction fetch) and lets each run at its own
+// occupancy.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -48,19 +54,17 @@ __device__ __forceinline__ long long find_surface_g(const int64_t* off, long lon
 }
 
 template <bool BATES>
-__global__ void __launch_bounds__(128, OPE_GRAD_MINB) k_price_grad(const ope_contract* __restrict__ con, long long n,
-                                                    const int64_t* __restrict__ surf_off, long long n_surf,
-                                                    const int32_t* __restrict__ param_idx,
-                                                    const int32_t* __restrict__ surf_mask,
-                                                    const double* __restrict__ params, double tol,
-                                                    double* __restrict__ out_price, double* __restrict__ out_grad,
-                                                    double* integ, double* ginteg, unsigned int* done,
-                                                    unsigned long long* head) {
+__global__ void __launch_bounds__(128, OPE_GRAD_MINB) k_grad_backward(const ope_contract* __restrict__ con, long long n,
+                                                      const int64_t* __restrict__ surf_off, long long n_surf,
+                                                      const int32_t* __restrict__ param_idx,
+                                                      const int32_t* __restrict__ surf_mask,
+                                                      const double* __restrict__ params,
+                                                      const int32_t* __restrict__ nbis,
+                                                      const double* __restrict__ panels, double* __restrict__ ginteg,
+                                                      unsigned long long* head) {
     constexpr int DIM = BATES ? 8 : 5;
-    extern __shared__ PanelStore smem_panels[];
     __shared__ double s_norm[4][16];  // per warp: the P1 normaliser's dLog CF(-i)/dp (complex, DIM <= 8)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    PanelStore& L = smem_panels[warp];
     const LaneRule R = lane_rule(lane);
     const unsigned long long n_units = 2ull * (unsigned long long)n;
     while (true) {
@@ -84,18 +88,11 @@ __global__ void __launch_bounds__(128, OPE_GRAD_MINB) k_price_grad(const ope_con
 #pragma unroll
         for (int i = 0; i < DIM; ++i) pl[i] = __ldg(p + i);
         const ope_contract* cp = con + c;
-        const double S = __ldg(&cp->spot), K = __ldg(&cp->strike), T = __ldg(&cp->expiry), r = __ldg(&cp->rate),
-                     q = __ldg(&cp->div_yield);
-        const int ot = __ldg(&cp->opt_type);
-        const CfConsts C = make_consts(S, K, T, r, pl, BATES, which);
-        int nb;
-        const double I = gk_integrate_warp<BATES>(C, tol, L, lane, R, &nb);
-        const int len = nb + 1;
-
-        // derivative integral over the final panel set; for P1 one extra work
-        // item evaluates the normaliser's dLog CF(-i)/dp (u = 0), so that the
-        // kernel holds ONE inlined copy of exponent_and_grad
+        const CfConsts C = make_consts(__ldg(&cp->spot), __ldg(&cp->strike), __ldg(&cp->expiry), __ldg(&cp->rate),
+                                       pl, BATES, which);
         const GradParams G = make_grad_params(pl, BATES);
+        const int len = __ldg(nbis + unit) + 1;
+        const double* P = panels + unit * (2 * kMaxPanels);
         double acc[DIM];
 #pragma unroll
         for (int k = 0; k < DIM; ++k) acc[k] = 0.0;
@@ -111,7 +108,7 @@ __global__ void __launch_bounds__(128, OPE_GRAD_MINB) k_price_grad(const ope_con
                 const bool normaliser = idx == total;
                 double tn = 0.0, hw = 0.0, u = 0.0;
                 if (!normaliser) {
-                    const double a = L.a[pi], b = L.b[pi];
+                    const double a = __ldg(P + 2 * pi), b = __ldg(P + 2 * pi + 1);
                     const double cc = 0.5 * (a + b), h = 0.5 * (b - a);
                     tn = __dadd_rn(cc, __dmul_rn(h, xj));
                     hw = h * wj;
@@ -141,27 +138,31 @@ __global__ void __launch_bounds__(128, OPE_GRAD_MINB) k_price_grad(const ope_con
             __syncwarp();
         }
         if (lane == 0) {
-            integ[2 * c + which] = I;
 #pragma unroll
-            for (int k = 0; k < DIM; ++k) ginteg[(2 * c + which) * DIM + k] = acc[k];
-            __threadfence();
-            const unsigned int prev = atomicAdd(done + c, 1u);
-            if (prev == 1u) {
-                __threadfence();
-                const int o = 1 - which;
-                const double other = __ldcg(integ + 2 * c + o);
-                const double i1 = which == 0 ? I : other, i2 = which == 0 ? other : I;
-                out_price[c] = finish_price(S, K, T, r, q, ot, i1, i2);
-                const double PI = 3.14159265358979323846;
-                const double seq = S * exp(-q * T), ker = K * exp(-r * T);
-#pragma unroll
-                for (int k = 0; k < DIM; ++k) {
-                    const double og = __ldcg(ginteg + (2 * c + o) * DIM + k);
-                    const double d1 = which == 0 ? acc[k] : og, d2 = which == 0 ? og : acc[k];
-                    out_grad[c * DIM + k] = seq * (d1 / PI) - ker * (d2 / PI);
-                }
-            }
+            for (int k = 0; k < DIM; ++k) ginteg[unit * DIM + k] = acc[k];
         }
+    }
+}
+
+// ad.rs:713-730 per contract; contracts of masked surfaces are left untouched.
+template <int DIM>
+__global__ void k_grad_combine(const ope_contract* __restrict__ con, long long n, const int64_t* __restrict__ surf_off,
+                               long long n_surf, const int32_t* __restrict__ param_idx,
+                               const int32_t* __restrict__ surf_mask, const double* __restrict__ ginteg,
+                               double* __restrict__ out_grad) {
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    if (surf_mask) {
+        const long long s = param_idx ? (long long)param_idx[c] : (n_surf > 1 ? find_surface_g(surf_off, n_surf, c) : 0);
+        if (surf_mask[s] == 0) return;
+    }
+    const ope_contract& cp = con[c];
+    const double PI = 3.14159265358979323846;
+    const double seq = cp.spot * exp(-cp.div_yield * cp.expiry), ker = cp.strike * exp(-cp.rate * cp.expiry);
+#pragma unroll
+    for (int k = 0; k < DIM; ++k) {
+        const double d1 = ginteg[(2 * c) * DIM + k], d2 = ginteg[(2 * c + 1) * DIM + k];
+        out_grad[c * DIM + k] = seq * (d1 / PI) - ker * (d2 / PI);
     }
 }
 
@@ -179,31 +180,52 @@ int grad_grid(K kernel, size_t smem, unsigned long long need, int* grid) {
 }  // namespace
 
 size_t grad_scratch_bytes(size_t n, int dim) {
-    return price_scratch_bytes(n) + align_up(2 * n * dim * sizeof(double), 256);
+    return price_scratch_bytes(n) + align_up(2 * n * sizeof(int32_t), 256) +
+           align_up(2 * n * 2 * kMaxPanels * sizeof(double), 256) + align_up(2 * n * dim * sizeof(double), 256) + 256;
 }
 
 int launch_price_grad(int model, const ope_contract* con, size_t n, const int64_t* surf_offsets, size_t n_surf,
                       const int32_t* param_idx, const double* params, double tol, double* out_price,
                       double* out_grad, void* scratch, cudaStream_t st, const int32_t* surf_mask) {
     if (n == 0) return OPE_OK;
-    const PriceScratch s = carve_price_scratch(scratch, n);
-    double* ginteg = reinterpret_cast<double*>(static_cast<char*>(scratch) + price_scratch_bytes(n));
-    OPE_CHECK(cudaMemsetAsync(s.done, 0, n * sizeof(unsigned int), st));
-    OPE_CHECK(cudaMemsetAsync(s.head, 0, sizeof(unsigned long long), st));
-    const size_t smem = 4 * sizeof(PanelStore);
+    const int dim = param_stride(model);
+    char* p = static_cast<char*>(scratch);
+    const PriceScratch s = carve_price_scratch(p, n);
+    p += price_scratch_bytes(n);
+    int32_t* nbis = reinterpret_cast<int32_t*>(p);
+    p += align_up(2 * n * sizeof(int32_t), 256);
+    double* panels = reinterpret_cast<double*>(p);
+    p += align_up(2 * n * 2 * kMaxPanels * sizeof(double), 256);
+    double* ginteg = reinterpret_cast<double*>(p);
+    p += align_up(2 * n * dim * sizeof(double), 256);
+    unsigned long long* head = reinterpret_cast<unsigned long long*>(p);
+    // 1. prices and the final panel lists
+    OPE_TRY(launch_price_persistent(model, con, n, surf_offsets, n_surf, param_idx, params, tol, out_price, s, st,
+                                    nbis, surf_mask, panels));
+    // 2. the backward pass over the stored panels
+    OPE_CHECK(cudaMemsetAsync(head, 0, sizeof(unsigned long long), st));
     const unsigned long long need = (2ull * n + 3) / 4;
     int grid = 0;
     if (model == OPE_MODEL_BATES) {
-        OPE_TRY(grad_grid(k_price_grad<true>, smem, need, &grid));
-        k_price_grad<true><<<grid, 128, smem, st>>>(con, (long long)n, surf_offsets, (long long)n_surf, param_idx,
-                                                    surf_mask, params, tol, out_price, out_grad, s.integ, ginteg, s.done, s.head);
+        OPE_TRY(grad_grid(k_grad_backward<true>, 0, need, &grid));
+        k_grad_backward<true><<<grid, 128, 0, st>>>(con, (long long)n, surf_offsets, (long long)n_surf, param_idx,
+                                                    surf_mask, params, nbis, panels, ginteg, head);
     } else {
-        OPE_TRY(grad_grid(k_price_grad<false>, smem, need, &grid));
-        k_price_grad<false><<<grid, 128, smem, st>>>(con, (long long)n, surf_offsets, (long long)n_surf, param_idx,
-                                                     surf_mask, params, tol, out_price, out_grad, s.integ, ginteg, s.done, s.head);
+        OPE_TRY(grad_grid(k_grad_backward<false>, 0, need, &grid));
+        k_grad_backward<false><<<grid, 128, 0, st>>>(con, (long long)n, surf_offsets, (long long)n_surf, param_idx,
+                                                     surf_mask, params, nbis, panels, ginteg, head);
     }
     OPE_CHECK(cudaGetLastError());
-    tctx().launches += 1;
+    // 3. the per-contract combination
+    const unsigned cb = (unsigned)((n + 127) / 128);
+    if (dim == 8)
+        k_grad_combine<8><<<cb, 128, 0, st>>>(con, (long long)n, surf_offsets, (long long)n_surf, param_idx, surf_mask,
+                                              ginteg, out_grad);
+    else
+        k_grad_combine<5><<<cb, 128, 0, st>>>(con, (long long)n, surf_offsets, (long long)n_surf, param_idx, surf_mask,
+                                              ginteg, out_grad);
+    OPE_CHECK(cudaGetLastError());
+    tctx().launches += 2;
     return OPE_OK;
 }
 

@@ -65,10 +65,12 @@ PriceScratch carve_price_scratch(void* base, size_t n);
 // when param_idx is non-NULL, else the surface of c under surf_offsets
 // (n_surf + 1 entries), else 0.  With surf_mask non-NULL, units whose p(c)
 // has surf_mask[p(c)] == 0 are skipped (their outputs are left untouched).
+// panels_out (non-NULL): each integral's final live-panel list as (a, b)
+// pairs at panels_out + (2c + which) * 2 * kMaxPanels (kMaxPanels = 200).
 int launch_price_persistent(int model, const ope_contract* con, size_t n, const int64_t* surf_offsets,
                             size_t n_surf, const int32_t* param_idx, const double* params, double tol, double* out,
                             const PriceScratch& s, cudaStream_t st, int32_t* nbis_out = nullptr,
-                            const int32_t* surf_mask = nullptr);
+                            const int32_t* surf_mask = nullptr, double* panels_out = nullptr);
 // Price + reverse-mode parameter gradient (adjoint.cu); `scratch` must hold
 // grad_scratch_bytes(n, dim) bytes; out_grad is n x dim (dim 5 or 8).
 size_t grad_scratch_bytes(size_t n, int dim);

@@ -63,11 +63,14 @@ __device__ __forceinline__ ContractView load_contract(const ope_contract* con, l
 }
 
 // Integrate unit (contract c, integral `which`) and, if it completes the
-// contract, write the price.
-template <bool BATES>
+// contract, write the price.  SAVE: also store the final live-panel list,
+// (a, b) pairs, in panels[(2c + which) * kMaxPanels ...] (the adjoint's
+// backward pass integrates over it).
+template <bool BATES, bool SAVE>
 __device__ __forceinline__ void run_unit(long long c, int which, const ope_contract* con, const double* p,
                                          double tol, double* out, double* integ, unsigned int* done,
-                                         int32_t* nbis_out, PanelStore& L, int lane, const LaneRule& R) {
+                                         int32_t* nbis_out, double* panels, PanelStore& L, int lane,
+                                         const LaneRule& R) {
     const ContractView v = load_contract(con, c);
     double pl[8];
 #pragma unroll
@@ -75,6 +78,14 @@ __device__ __forceinline__ void run_unit(long long c, int which, const ope_contr
     const CfConsts C = make_consts(v.s, v.k, v.t, v.r, pl, BATES, which);
     int nb;
     const double I = gk_integrate_warp<BATES>(C, tol, L, lane, R, &nb);
+    if (SAVE) {
+        double* dst = panels + (size_t)(2 * c + which) * (2 * kMaxPanels);
+        for (int i = lane; i <= nb; i += 32) {
+            dst[2 * i] = L.a[i];
+            dst[2 * i + 1] = L.b[i];
+        }
+        __syncwarp();  // the list is read before the next unit rewrites it
+    }
     if (lane == 0) {
         if (nbis_out) nbis_out[2 * c + which] = nb;
         integ[2 * c + which] = I;
@@ -102,7 +113,7 @@ __device__ __forceinline__ long long find_surface(const int64_t* off, long long 
 
 // Every warp pulls units from the device queue until it drains; the grid is
 // the resident capacity of the GPU, or fewer warps than units for small calls.
-template <bool BATES>
+template <bool BATES, bool SAVE>
 __global__ void __launch_bounds__(OPE_KERNEL_WARPS * 32, OPE_KERNEL_MINB) k_price_persistent(const ope_contract* __restrict__ con, long long n,
                                                           const int64_t* __restrict__ surf_off, long long n_surf,
                                                           const int32_t* __restrict__ param_idx,
@@ -110,7 +121,7 @@ __global__ void __launch_bounds__(OPE_KERNEL_WARPS * 32, OPE_KERNEL_MINB) k_pric
                                                           const double* __restrict__ params, double tol,
                                                           double* __restrict__ out, double* integ,
                                                           unsigned int* done, unsigned long long* head,
-                                                          int32_t* nbis_out) {
+                                                          int32_t* nbis_out, double* panels) {
     extern __shared__ PanelStore smem_panels[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const LaneRule R = lane_rule(lane);
@@ -131,8 +142,8 @@ __global__ void __launch_bounds__(OPE_KERNEL_WARPS * 32, OPE_KERNEL_MINB) k_pric
                 atomicMax(head, 2ull * (unsigned long long)__ldg(surf_off + s + 1));
             continue;
         }
-        run_unit<BATES>(c, (int)(unit & 1), con, params + s * stride, tol, out, integ, done, nbis_out,
-                        smem_panels[warp], lane, R);
+        run_unit<BATES, SAVE>(c, (int)(unit & 1), con, params + s * stride, tol, out, integ, done, nbis_out,
+                              panels, smem_panels[warp], lane, R);
     }
 }
 
@@ -146,31 +157,40 @@ int persistent_grid(K kernel, int threads, size_t smem, int* grid) {
     return OPE_OK;
 }
 
+template <bool BATES, bool SAVE>
+int launch_impl(const ope_contract* con, size_t n, const int64_t* surf_offsets, size_t n_surf,
+                const int32_t* param_idx, const double* params, double tol, double* out, const PriceScratch& s,
+                cudaStream_t st, int32_t* nbis_out, const int32_t* surf_mask, double* panels) {
+    const int warps = OPE_KERNEL_WARPS, threads = warps * 32;
+    const size_t smem = warps * sizeof(PanelStore);
+    int grid = 0;
+    OPE_TRY(persistent_grid(k_price_persistent<BATES, SAVE>, threads, smem, &grid));
+    const unsigned long long need = (2ull * n + warps - 1) / warps;
+    grid = (int)std::min<unsigned long long>((unsigned long long)grid, need);
+    k_price_persistent<BATES, SAVE><<<grid, threads, smem, st>>>(con, (long long)n, surf_offsets, (long long)n_surf,
+                                                                 param_idx, surf_mask, params, tol, out, s.integ,
+                                                                 s.done, s.head, nbis_out, panels);
+    OPE_CHECK(cudaGetLastError());
+    return OPE_OK;
+}
+
 }  // namespace
 
 int launch_price_persistent(int model, const ope_contract* con, size_t n, const int64_t* surf_offsets,
                             size_t n_surf, const int32_t* param_idx, const double* params, double tol, double* out,
-                            const PriceScratch& s, cudaStream_t st, int32_t* nbis_out, const int32_t* surf_mask) {
+                            const PriceScratch& s, cudaStream_t st, int32_t* nbis_out, const int32_t* surf_mask,
+                            double* panels_out) {
     if (n == 0) return OPE_OK;
     OPE_CHECK(cudaMemsetAsync(s.done, 0, n * sizeof(unsigned int), st));
     OPE_CHECK(cudaMemsetAsync(s.head, 0, sizeof(unsigned long long), st));
-    const int warps = OPE_KERNEL_WARPS, threads = warps * 32;
-    const size_t smem = warps * sizeof(PanelStore);
-    int grid = 0;
-    if (model == OPE_MODEL_BATES) {
-        OPE_TRY(persistent_grid(k_price_persistent<true>, threads, smem, &grid));
-        const unsigned long long need = (2ull * n + warps - 1) / warps;
-        grid = (int)std::min<unsigned long long>((unsigned long long)grid, need);
-        k_price_persistent<true><<<grid, threads, smem, st>>>(con, (long long)n, surf_offsets, (long long)n_surf,
-                                                              param_idx, surf_mask, params, tol, out, s.integ, s.done, s.head, nbis_out);
+    const bool bates = model == OPE_MODEL_BATES;
+    if (panels_out) {
+        OPE_TRY((bates ? launch_impl<true, true> : launch_impl<false, true>)(
+            con, n, surf_offsets, n_surf, param_idx, params, tol, out, s, st, nbis_out, surf_mask, panels_out));
     } else {
-        OPE_TRY(persistent_grid(k_price_persistent<false>, threads, smem, &grid));
-        const unsigned long long need = (2ull * n + warps - 1) / warps;
-        grid = (int)std::min<unsigned long long>((unsigned long long)grid, need);
-        k_price_persistent<false><<<grid, threads, smem, st>>>(con, (long long)n, surf_offsets, (long long)n_surf,
-                                                               param_idx, surf_mask, params, tol, out, s.integ, s.done, s.head, nbis_out);
+        OPE_TRY((bates ? launch_impl<true, false> : launch_impl<false, false>)(
+            con, n, surf_offsets, n_surf, param_idx, params, tol, out, s, st, nbis_out, surf_mask, nullptr));
     }
-    OPE_CHECK(cudaGetLastError());
     tctx().launches += 1;
     return OPE_OK;
 }
