@@ -58,10 +58,8 @@ __global__ void __launch_bounds__(128, OPE_GRAD_MINB) k_grad_backward(const ope_
                                                       const int64_t* __restrict__ surf_off, long long n_surf,
                                                       const int32_t* __restrict__ param_idx,
                                                       const int32_t* __restrict__ surf_mask,
-                                                      const double* __restrict__ params,
-                                                      const int32_t* __restrict__ nbis,
-                                                      const double* __restrict__ panels, double* __restrict__ ginteg,
-                                                      unsigned long long* head) {
+                                                      const double* __restrict__ params, PanelSink src,
+                                                      double* __restrict__ ginteg, unsigned long long* head) {
     constexpr int DIM = BATES ? 8 : 5;
     __shared__ double s_norm[4][16];  // per warp: the P1 normaliser's dLog CF(-i)/dp (complex, DIM <= 8)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -91,8 +89,9 @@ __global__ void __launch_bounds__(128, OPE_GRAD_MINB) k_grad_backward(const ope_
         const CfConsts C = make_consts(__ldg(&cp->spot), __ldg(&cp->strike), __ldg(&cp->expiry), __ldg(&cp->rate),
                                        pl, BATES, which);
         const GradParams G = make_grad_params(pl, BATES);
-        const int len = __ldg(nbis + unit) + 1;
-        const double* P = panels + unit * (2 * kMaxPanels);
+        const size_t pidx = (size_t)unit * src.n_slots + (src.slot ? __ldg(src.slot + s) : 0);
+        const int len = __ldg(src.nbis + pidx) + 1;
+        const double* P = src.panels + pidx * (2 * kMaxPanels);
         double acc[DIM];
 #pragma unroll
         for (int k = 0; k < DIM; ++k) acc[k] = 0.0;
@@ -180,43 +179,27 @@ int grad_grid(K kernel, size_t smem, unsigned long long need, int* grid) {
 }  // namespace
 
 size_t grad_scratch_bytes(size_t n, int dim) {
-    return price_scratch_bytes(n) + align_up(2 * n * sizeof(int32_t), 256) +
-           align_up(2 * n * 2 * kMaxPanels * sizeof(double), 256) + align_up(2 * n * dim * sizeof(double), 256) + 256;
+    return price_scratch_bytes(n) + panel_sink_bytes(n, 1) + align_up(2 * n * dim * sizeof(double), 256) + 256;
 }
 
-int launch_price_grad(int model, const ope_contract* con, size_t n, const int64_t* surf_offsets, size_t n_surf,
-                      const int32_t* param_idx, const double* params, double tol, double* out_price,
-                      double* out_grad, void* scratch, cudaStream_t st, const int32_t* surf_mask) {
+int launch_grad_backward(int model, const ope_contract* con, size_t n, const int64_t* surf_offsets, size_t n_surf,
+                         const int32_t* param_idx, const double* params, const PanelSink& src, double* ginteg,
+                         unsigned long long* head, double* out_grad, cudaStream_t st, const int32_t* surf_mask) {
     if (n == 0) return OPE_OK;
     const int dim = param_stride(model);
-    char* p = static_cast<char*>(scratch);
-    const PriceScratch s = carve_price_scratch(p, n);
-    p += price_scratch_bytes(n);
-    int32_t* nbis = reinterpret_cast<int32_t*>(p);
-    p += align_up(2 * n * sizeof(int32_t), 256);
-    double* panels = reinterpret_cast<double*>(p);
-    p += align_up(2 * n * 2 * kMaxPanels * sizeof(double), 256);
-    double* ginteg = reinterpret_cast<double*>(p);
-    p += align_up(2 * n * dim * sizeof(double), 256);
-    unsigned long long* head = reinterpret_cast<unsigned long long*>(p);
-    // 1. prices and the final panel lists
-    OPE_TRY(launch_price_persistent(model, con, n, surf_offsets, n_surf, param_idx, params, tol, out_price, s, st,
-                                    nbis, surf_mask, panels));
-    // 2. the backward pass over the stored panels
     OPE_CHECK(cudaMemsetAsync(head, 0, sizeof(unsigned long long), st));
     const unsigned long long need = (2ull * n + 3) / 4;
     int grid = 0;
     if (model == OPE_MODEL_BATES) {
         OPE_TRY(grad_grid(k_grad_backward<true>, 0, need, &grid));
         k_grad_backward<true><<<grid, 128, 0, st>>>(con, (long long)n, surf_offsets, (long long)n_surf, param_idx,
-                                                    surf_mask, params, nbis, panels, ginteg, head);
+                                                    surf_mask, params, src, ginteg, head);
     } else {
         OPE_TRY(grad_grid(k_grad_backward<false>, 0, need, &grid));
         k_grad_backward<false><<<grid, 128, 0, st>>>(con, (long long)n, surf_offsets, (long long)n_surf, param_idx,
-                                                     surf_mask, params, nbis, panels, ginteg, head);
+                                                     surf_mask, params, src, ginteg, head);
     }
     OPE_CHECK(cudaGetLastError());
-    // 3. the per-contract combination
     const unsigned cb = (unsigned)((n + 127) / 128);
     if (dim == 8)
         k_grad_combine<8><<<cb, 128, 0, st>>>(con, (long long)n, surf_offsets, (long long)n_surf, param_idx, surf_mask,
@@ -227,6 +210,26 @@ int launch_price_grad(int model, const ope_contract* con, size_t n, const int64_
     OPE_CHECK(cudaGetLastError());
     tctx().launches += 2;
     return OPE_OK;
+}
+
+int launch_price_grad(int model, const ope_contract* con, size_t n, const int64_t* surf_offsets, size_t n_surf,
+                      const int32_t* param_idx, const double* params, double tol, double* out_price,
+                      double* out_grad, void* scratch, cudaStream_t st, const int32_t* surf_mask) {
+    if (n == 0) return OPE_OK;
+    const int dim = param_stride(model);
+    char* p = static_cast<char*>(scratch);
+    const PriceScratch s = carve_price_scratch(p, n);
+    p += price_scratch_bytes(n);
+    const PanelSink sink = carve_panel_sink(p, n, 1, nullptr);
+    p += panel_sink_bytes(n, 1);
+    double* ginteg = reinterpret_cast<double*>(p);
+    p += align_up(2 * n * dim * sizeof(double), 256);
+    unsigned long long* head = reinterpret_cast<unsigned long long*>(p);
+    // 1. prices and the final panel lists, 2. the backward pass and combine
+    OPE_TRY(launch_price_persistent(model, con, n, surf_offsets, n_surf, param_idx, params, tol, out_price, s, st,
+                                    nullptr, surf_mask, &sink));
+    return launch_grad_backward(model, con, n, surf_offsets, n_surf, param_idx, params, sink, ginteg, head, out_grad,
+                                st, surf_mask);
 }
 
 }  // namespace ope

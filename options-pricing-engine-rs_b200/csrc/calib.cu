@@ -17,7 +17,11 @@
 // fails contributes a zero residual (calibration.rs:577-580) and a zero
 // Jacobian row.  J at a given p is deterministic, so it is recomputed only
 // after an accepted step (the reference recomputes the same J after a
-// rejected or out-of-bounds step).
+// rejected or out-of-bounds step).  Every pricing of the loop (the initial
+// one at p0, each trial) stores its integrals' final panel lists in one of
+// two slots per surface; an accepted trial's slot becomes the current one,
+// so the Jacobian at the new p is only the adjoint's backward pass over
+// lists that already exist, not a second pricing.
 //
 // Optional per surface (CalibExtra): a Tikhonov prior, added as dim pseudo
 // rows (p_k - prior_k) / scale_k of weight sqrt(reg_weight) to the SSE, J'J
@@ -74,7 +78,10 @@ struct LMDev {
     double* ptrial;  // ns x dim: trial parameters
     int32_t* jmask;  // ns: surfaces needing J this iteration
     int32_t* tmask;  // ns: surfaces with a trial step this iteration
-    double* price;   // nq
+    double* price;   // nq: model prices at the current parameters
+    double* price_trial;  // nq: model prices at the trial parameters
+    int32_t* jslot;  // ns: panel-list slot of the current parameters
+    int32_t* pslot;  // ns: panel-list slot the next pricing writes
     double* pgrad;   // nq x dim
     double* res;     // nq
     double* res_new; // nq
@@ -208,6 +215,8 @@ __global__ void k_lm_init(LMDev D, const double* p0) {
     S.trial = 0;
     D.jmask[s] = 1;
     D.tmask[s] = 1;  // the initial pricing pass prices every surface at p0
+    D.jslot[s] = 0;  // ... into slot 0, the current parameters' slot
+    D.pslot[s] = 0;
 }
 
 // IV residual of every quote whose surface is selected by `mask`
@@ -352,7 +361,10 @@ __global__ void k_lm_accept(LMDev D) {
     const double sse_new = add_reg_sse(D, s, S.p_new, warp_sum(part));
     const bool accept = sse_new < S.sse;
     if (accept)
-        for (int64_t i = D.off[s] + lane; i < D.off[s + 1]; i += 32) D.res[i] = D.res_new[i];
+        for (int64_t i = D.off[s] + lane; i < D.off[s + 1]; i += 32) {
+            D.res[i] = D.res_new[i];
+            D.price[i] = D.price_trial[i];
+        }
     if (lane != 0) return;
     const int dim = D.dim;
     D.tmask[s] = 0;
@@ -364,6 +376,8 @@ __global__ void k_lm_accept(LMDev D) {
         if (D.group) atomicMin(D.gbest + D.group[s], (unsigned long long)__double_as_longlong(sse_new));
         S.need_jac = 1;
         D.jmask[s] = 1;
+        D.jslot[s] = D.pslot[s];  // the trial's panel lists are now the current ones
+        D.pslot[s] = 1 - D.pslot[s];
         double sn = 0.0;
         for (int k = 0; k < dim; ++k) sn += S.dp[k] * S.dp[k];
         if (sqrt(sn) < kTolParams) { S.status = LM_CONVERGED; return; }  // J at the final p still due
@@ -385,7 +399,11 @@ __global__ void k_lm_sse0(LMDev D) {
         part += t * t;
     }
     const double sse = warp_sum(part);
-    if (lane == 0) { D.st[s].sse = add_reg_sse(D, s, D.st[s].p, sse); D.tmask[s] = 0; }
+    if (lane == 0) {
+        D.st[s].sse = add_reg_sse(D, s, D.st[s].p, sse);
+        D.tmask[s] = 0;
+        D.pslot[s] = 1 - D.jslot[s];  // trials write the other slot
+    }
 }
 
 // Count surfaces still iterating and drive the graph's WHILE condition.
@@ -472,8 +490,8 @@ thread_local CalibGraph g_lm_graph;
 
 struct Layout {
     size_t total;
-    size_t q, iv, w, off, sidx, st, pcur, ptrial, jmask, tmask, price, pgrad, res, res_new, jrow, counters, out,
-        prior, regw, group, gbest, scratch;
+    size_t q, iv, w, off, sidx, st, pcur, ptrial, jmask, tmask, price, price_trial, jslot, pslot, pgrad, res, res_new,
+        jrow, counters, out, prior, regw, group, gbest, sink, ginteg, bhead, scratch;
 };
 
 Layout layout(size_t nq, size_t ns, int dim) {
@@ -491,6 +509,9 @@ Layout layout(size_t nq, size_t ns, int dim) {
     L.jmask = take(ns * sizeof(int32_t));
     L.tmask = take(ns * sizeof(int32_t));
     L.price = take(nq * sizeof(double));
+    L.price_trial = take(nq * sizeof(double));
+    L.jslot = take(ns * sizeof(int32_t));
+    L.pslot = take(ns * sizeof(int32_t));
     L.pgrad = take(nq * dim * sizeof(double));
     L.res = take(nq * sizeof(double));
     L.res_new = take(nq * sizeof(double));
@@ -501,7 +522,10 @@ Layout layout(size_t nq, size_t ns, int dim) {
     L.regw = take(ns * sizeof(double));
     L.group = take(ns * sizeof(int32_t));
     L.gbest = take(ns * sizeof(unsigned long long));
-    L.scratch = take(grad_scratch_bytes(nq, dim));
+    L.sink = take(panel_sink_bytes(nq, 2));
+    L.ginteg = take(2 * nq * dim * sizeof(double));
+    L.bhead = take(sizeof(unsigned long long));
+    L.scratch = take(price_scratch_bytes(nq));
     L.total = o;
     return L;
 }
@@ -522,6 +546,9 @@ LMDev make_dev(char* base, const Layout& L, int nq, int ns, int dim) {
     D.jmask = reinterpret_cast<int32_t*>(base + L.jmask);
     D.tmask = reinterpret_cast<int32_t*>(base + L.tmask);
     D.price = reinterpret_cast<double*>(base + L.price);
+    D.price_trial = reinterpret_cast<double*>(base + L.price_trial);
+    D.jslot = reinterpret_cast<int32_t*>(base + L.jslot);
+    D.pslot = reinterpret_cast<int32_t*>(base + L.pslot);
     D.pgrad = reinterpret_cast<double*>(base + L.pgrad);
     D.res = reinterpret_cast<double*>(base + L.res);
     D.res_new = reinterpret_cast<double*>(base + L.res_new);
@@ -534,9 +561,18 @@ LMDev make_dev(char* base, const Layout& L, int nq, int ns, int dim) {
     return D;
 }
 
-int launch_jac(int model, const LMDev& D, char* base, const Layout& L, double tol, cudaStream_t st) {
-    OPE_TRY(launch_price_grad(model, D.q, D.nq, D.off, D.ns, nullptr, D.pcur, tol, D.price, D.pgrad,
-                              base + L.scratch, st, D.jmask));
+// The pricing launches' panel-list sink, writing each surface's pslot.
+PanelSink pricing_sink(const LMDev& D, char* base, const Layout& L) {
+    return carve_panel_sink(base + L.sink, D.nq, 2, D.pslot);
+}
+
+// d price / d p at the current parameters of the surfaces in jmask: the
+// adjoint's backward pass over the panel lists of the current slot.
+int launch_jac(int model, const LMDev& D, char* base, const Layout& L, cudaStream_t st) {
+    const PanelSink src = carve_panel_sink(base + L.sink, D.nq, 2, D.jslot);
+    OPE_TRY(launch_grad_backward(model, D.q, D.nq, D.off, D.ns, nullptr, D.pcur, src,
+                                 reinterpret_cast<double*>(base + L.ginteg),
+                                 reinterpret_cast<unsigned long long*>(base + L.bhead), D.pgrad, st, D.jmask));
     k_lm_jrows<<<(D.nq + 127) / 128, 128, 0, st>>>(D);
     OPE_CHECK(cudaGetLastError());
     tctx().launches += 1;
@@ -547,12 +583,13 @@ int launch_jac(int model, const LMDev& D, char* base, const Layout& L, double to
 int enqueue_body(int model, const LMDev& D, char* base, const Layout& L, double tol, cudaStream_t st,
                  cudaGraphConditionalHandle handle) {
     const int warps_blocks = (D.ns * 32 + 127) / 128;
-    OPE_TRY(launch_jac(model, D, base, L, tol, st));
+    OPE_TRY(launch_jac(model, D, base, L, st));
     k_lm_step<<<warps_blocks, 128, 0, st>>>(D);
     OPE_CHECK(cudaGetLastError());
-    OPE_TRY(launch_price_persistent(model, D.q, D.nq, D.off, D.ns, nullptr, D.ptrial, tol, D.price,
-                                    carve_price_scratch(base + L.scratch, D.nq), st, nullptr, D.tmask));
-    k_lm_residuals<<<(D.nq + 127) / 128, 128, 0, st>>>(D, D.tmask, D.price, D.res_new);
+    const PanelSink sink = pricing_sink(D, base, L);
+    OPE_TRY(launch_price_persistent(model, D.q, D.nq, D.off, D.ns, nullptr, D.ptrial, tol, D.price_trial,
+                                    carve_price_scratch(base + L.scratch, D.nq), st, nullptr, D.tmask, &sink));
+    k_lm_residuals<<<(D.nq + 127) / 128, 128, 0, st>>>(D, D.tmask, D.price_trial, D.res_new);
     OPE_CHECK(cudaGetLastError());
     k_lm_accept<<<warps_blocks, 128, 0, st>>>(D);
     OPE_CHECK(cudaGetLastError());
@@ -673,8 +710,9 @@ int calib_enqueue(int model, const ope_contract* quotes, const double* iv_market
     // initial state and residuals at p0 (calibration.rs:472-475)
     k_lm_init<<<((int)ns + 127) / 128, 128, 0, st>>>(D, p0_dev);
     OPE_CHECK(cudaGetLastError());
+    const PanelSink sink = pricing_sink(D, base, L);
     OPE_TRY(launch_price_persistent(model, D.q, nq, D.off, ns, nullptr, D.pcur, tol, D.price,
-                                    carve_price_scratch(base + L.scratch, nq), st, nullptr, D.tmask));
+                                    carve_price_scratch(base + L.scratch, nq), st, nullptr, D.tmask, &sink));
     k_lm_residuals<<<((int)nq + 127) / 128, 128, 0, st>>>(D, nullptr, D.price, D.res);
     OPE_CHECK(cudaGetLastError());
     k_lm_sse0<<<((int)ns * 32 + 127) / 128, 128, 0, st>>>(D);
@@ -698,7 +736,7 @@ int calib_enqueue(int model, const ope_contract* quotes, const double* iv_market
     }
     OPE_CHECK(cudaGraphLaunch(g.exec, st));
     // final Jacobian at the last accepted parameters, diagnostics
-    OPE_TRY(launch_jac(model, D, base, L, tol, st));
+    OPE_TRY(launch_jac(model, D, base, L, st));
     ope_calib_result* d_out = reinterpret_cast<ope_calib_result*>(base + L.out);
     k_lm_final<<<((int)ns * 32 + 127) / 128, 128, 0, st>>>(D, d_out);
     OPE_CHECK(cudaGetLastError());
@@ -792,7 +830,12 @@ int run_calib_jacobian(int model, const ope_contract* quotes, const double* iv_m
     OPE_CHECK(cudaMemcpyAsync(base + L.pcur, params, ns * dim * sizeof(double), cudaMemcpyHostToDevice, st));
     OPE_CHECK(cudaMemcpyAsync(base + L.jmask, ones.data(), ns * sizeof(int32_t), cudaMemcpyHostToDevice, st));
     LMDev D = make_dev(base, L, (int)nq, (int)ns, dim);
-    OPE_TRY(launch_jac(model, D, base, L, tol, st));
+    OPE_CHECK(cudaMemsetAsync(D.pslot, 0, ns * sizeof(int32_t), st));
+    OPE_CHECK(cudaMemsetAsync(D.jslot, 0, ns * sizeof(int32_t), st));
+    const PanelSink sink = pricing_sink(D, base, L);
+    OPE_TRY(launch_price_persistent(model, D.q, nq, D.off, ns, nullptr, D.pcur, tol, D.price,
+                                    carve_price_scratch(base + L.scratch, nq), st, nullptr, nullptr, &sink));
+    OPE_TRY(launch_jac(model, D, base, L, st));
     k_lm_residuals<<<((int)nq + 127) / 128, 128, 0, st>>>(D, nullptr, D.price, D.res);
     OPE_CHECK(cudaGetLastError());
     c.launches += 1;

@@ -65,12 +65,33 @@ PriceScratch carve_price_scratch(void* base, size_t n);
 // when param_idx is non-NULL, else the surface of c under surf_offsets
 // (n_surf + 1 entries), else 0.  With surf_mask non-NULL, units whose p(c)
 // has surf_mask[p(c)] == 0 are skipped (their outputs are left untouched).
-// panels_out (non-NULL): each integral's final live-panel list as (a, b)
-// pairs at panels_out + (2c + which) * 2 * kMaxPanels (kMaxPanels = 200).
+// Final live-panel lists of the integrals (the adjoint's backward pass runs
+// over them).  Unit u = 2c + which of parameter set p(c) uses slot k =
+// slot[p(c)] (slot NULL: 0) of n_slots: its bisection count is
+// nbis[u * n_slots + k] and its panels the (a, b) pairs at
+// panels + (u * n_slots + k) * 2 * kMaxPanels (kMaxPanels = 200).  Two slots
+// let a calibration keep the lists of its current parameters while a trial
+// step writes the other.
+struct PanelSink {
+    double* panels;
+    int32_t* nbis;
+    const int32_t* slot;
+    int n_slots;
+};
+size_t panel_sink_bytes(size_t n, int n_slots);  // panels + nbis for n contracts
+PanelSink carve_panel_sink(void* base, size_t n, int n_slots, const int32_t* slot);
+// sink (non-NULL): also store every priced integral's panel list there.
 int launch_price_persistent(int model, const ope_contract* con, size_t n, const int64_t* surf_offsets,
                             size_t n_surf, const int32_t* param_idx, const double* params, double tol, double* out,
                             const PriceScratch& s, cudaStream_t st, int32_t* nbis_out = nullptr,
-                            const int32_t* surf_mask = nullptr, double* panels_out = nullptr);
+                            const int32_t* surf_mask = nullptr, const PanelSink* sink = nullptr);
+// The adjoint's backward pass and combine (adjoint.cu) over panel lists a
+// pricing launch stored in `src`: out_grad (n x dim) = d price / d params.
+// ginteg: 2n x dim doubles; head: one zeroed-on-launch queue counter.
+int launch_grad_backward(int model, const ope_contract* con, size_t n, const int64_t* surf_offsets, size_t n_surf,
+                         const int32_t* param_idx, const double* params, const PanelSink& src, double* ginteg,
+                         unsigned long long* head, double* out_grad, cudaStream_t st,
+                         const int32_t* surf_mask = nullptr);
 // Price + reverse-mode parameter gradient (adjoint.cu); `scratch` must hold
 // grad_scratch_bytes(n, dim) bytes; out_grad is n x dim (dim 5 or 8).
 size_t grad_scratch_bytes(size_t n, int dim);

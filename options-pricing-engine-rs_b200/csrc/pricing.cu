@@ -32,6 +32,20 @@ size_t price_scratch_bytes(size_t n) {
     return align_up(2 * n * sizeof(double), 256) + align_up(n * sizeof(unsigned int), 256) + 256;
 }
 
+size_t panel_sink_bytes(size_t n, int n_slots) {
+    return align_up(2 * n * n_slots * 2 * kMaxPanels * sizeof(double), 256) + align_up(2 * n * n_slots * sizeof(int32_t), 256);
+}
+
+PanelSink carve_panel_sink(void* base, size_t n, int n_slots, const int32_t* slot) {
+    PanelSink k;
+    k.panels = static_cast<double*>(base);
+    k.nbis = reinterpret_cast<int32_t*>(static_cast<char*>(base) +
+                                        align_up(2 * n * n_slots * 2 * kMaxPanels * sizeof(double), 256));
+    k.slot = slot;
+    k.n_slots = n_slots;
+    return k;
+}
+
 PriceScratch carve_price_scratch(void* base, size_t n) {
     char* p = static_cast<char*>(base);
     PriceScratch s;
@@ -63,14 +77,14 @@ __device__ __forceinline__ ContractView load_contract(const ope_contract* con, l
 }
 
 // Integrate unit (contract c, integral `which`) and, if it completes the
-// contract, write the price.  SAVE: also store the final live-panel list,
-// (a, b) pairs, in panels[(2c + which) * kMaxPanels ...] (the adjoint's
-// backward pass integrates over it).
+// contract, write the price.  SAVE: also store the final live-panel list
+// and the bisection count in `sink` (slot `slot`), for the adjoint's backward
+// pass.
 template <bool BATES, bool SAVE>
 __device__ __forceinline__ void run_unit(long long c, int which, const ope_contract* con, const double* p,
                                          double tol, double* out, double* integ, unsigned int* done,
-                                         int32_t* nbis_out, double* panels, PanelStore& L, int lane,
-                                         const LaneRule& R) {
+                                         int32_t* nbis_out, const PanelSink& sink, int slot, PanelStore& L,
+                                         int lane, const LaneRule& R) {
     const ContractView v = load_contract(con, c);
     double pl[8];
 #pragma unroll
@@ -79,11 +93,13 @@ __device__ __forceinline__ void run_unit(long long c, int which, const ope_contr
     int nb;
     const double I = gk_integrate_warp<BATES>(C, tol, L, lane, R, &nb);
     if (SAVE) {
-        double* dst = panels + (size_t)(2 * c + which) * (2 * kMaxPanels);
+        const size_t idx = (size_t)(2 * c + which) * sink.n_slots + slot;
+        double* dst = sink.panels + idx * (2 * kMaxPanels);
         for (int i = lane; i <= nb; i += 32) {
             dst[2 * i] = L.a[i];
             dst[2 * i + 1] = L.b[i];
         }
+        if (lane == 0) sink.nbis[idx] = nb;
         __syncwarp();  // the list is read before the next unit rewrites it
     }
     if (lane == 0) {
@@ -121,7 +137,7 @@ __global__ void __launch_bounds__(OPE_KERNEL_WARPS * 32, OPE_KERNEL_MINB) k_pric
                                                           const double* __restrict__ params, double tol,
                                                           double* __restrict__ out, double* integ,
                                                           unsigned int* done, unsigned long long* head,
-                                                          int32_t* nbis_out, double* panels) {
+                                                          int32_t* nbis_out, PanelSink sink) {
     extern __shared__ PanelStore smem_panels[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const LaneRule R = lane_rule(lane);
@@ -142,8 +158,9 @@ __global__ void __launch_bounds__(OPE_KERNEL_WARPS * 32, OPE_KERNEL_MINB) k_pric
                 atomicMax(head, 2ull * (unsigned long long)__ldg(surf_off + s + 1));
             continue;
         }
+        const int slot = (SAVE && sink.slot) ? __ldg(sink.slot + s) : 0;
         run_unit<BATES, SAVE>(c, (int)(unit & 1), con, params + s * stride, tol, out, integ, done, nbis_out,
-                              panels, smem_panels[warp], lane, R);
+                              sink, slot, smem_panels[warp], lane, R);
     }
 }
 
@@ -160,7 +177,7 @@ int persistent_grid(K kernel, int threads, size_t smem, int* grid) {
 template <bool BATES, bool SAVE>
 int launch_impl(const ope_contract* con, size_t n, const int64_t* surf_offsets, size_t n_surf,
                 const int32_t* param_idx, const double* params, double tol, double* out, const PriceScratch& s,
-                cudaStream_t st, int32_t* nbis_out, const int32_t* surf_mask, double* panels) {
+                cudaStream_t st, int32_t* nbis_out, const int32_t* surf_mask, const PanelSink& sink) {
     const int warps = OPE_KERNEL_WARPS, threads = warps * 32;
     const size_t smem = warps * sizeof(PanelStore);
     int grid = 0;
@@ -169,7 +186,7 @@ int launch_impl(const ope_contract* con, size_t n, const int64_t* surf_offsets, 
     grid = (int)std::min<unsigned long long>((unsigned long long)grid, need);
     k_price_persistent<BATES, SAVE><<<grid, threads, smem, st>>>(con, (long long)n, surf_offsets, (long long)n_surf,
                                                                  param_idx, surf_mask, params, tol, out, s.integ,
-                                                                 s.done, s.head, nbis_out, panels);
+                                                                 s.done, s.head, nbis_out, sink);
     OPE_CHECK(cudaGetLastError());
     return OPE_OK;
 }
@@ -179,17 +196,18 @@ int launch_impl(const ope_contract* con, size_t n, const int64_t* surf_offsets, 
 int launch_price_persistent(int model, const ope_contract* con, size_t n, const int64_t* surf_offsets,
                             size_t n_surf, const int32_t* param_idx, const double* params, double tol, double* out,
                             const PriceScratch& s, cudaStream_t st, int32_t* nbis_out, const int32_t* surf_mask,
-                            double* panels_out) {
+                            const PanelSink* sink) {
     if (n == 0) return OPE_OK;
     OPE_CHECK(cudaMemsetAsync(s.done, 0, n * sizeof(unsigned int), st));
     OPE_CHECK(cudaMemsetAsync(s.head, 0, sizeof(unsigned long long), st));
     const bool bates = model == OPE_MODEL_BATES;
-    if (panels_out) {
+    if (sink) {
         OPE_TRY((bates ? launch_impl<true, true> : launch_impl<false, true>)(
-            con, n, surf_offsets, n_surf, param_idx, params, tol, out, s, st, nbis_out, surf_mask, panels_out));
+            con, n, surf_offsets, n_surf, param_idx, params, tol, out, s, st, nbis_out, surf_mask, *sink));
     } else {
+        const PanelSink none{nullptr, nullptr, nullptr, 1};
         OPE_TRY((bates ? launch_impl<true, false> : launch_impl<false, false>)(
-            con, n, surf_offsets, n_surf, param_idx, params, tol, out, s, st, nbis_out, surf_mask, nullptr));
+            con, n, surf_offsets, n_surf, param_idx, params, tol, out, s, st, nbis_out, surf_mask, none));
     }
     tctx().launches += 1;
     return OPE_OK;
