@@ -194,6 +194,29 @@ inline PricingResult bates_greeks_ad(double spot, double strike, double expiry, 
     return r;
 }
 
+// ad.rs heston_greeks_ad5: the joint five-parameter pass returns what
+// heston_greeks_ad returns (ad.rs:1295-1322), so it is the same computation.
+inline PricingResult heston_greeks_ad5(double spot, double strike, double expiry, double rate, double div_yield,
+                                       const HestonParams& params, OptionType opt_type) {
+    return heston_greeks_ad(spot, strike, expiry, rate, div_yield, params, opt_type);
+}
+
+struct BatesJumpSensitivities {  // ad.rs:866-871
+    double price, d_lambda, d_mu_j, d_sigma_j;
+};
+
+// ad.rs:882-895, through the reverse-mode adjoint
+inline BatesJumpSensitivities bates_jump_sensitivities_ad(double spot, double strike, double expiry, double rate,
+                                                          double div_yield, const HestonParams& heston, double lambda,
+                                                          double mu_j, double sigma_j, OptionType opt_type) {
+    const ope_contract c{spot, strike, expiry, rate, div_yield, 0.0, static_cast<int32_t>(opt_type), 0};
+    const double p[8] = {heston.v0, heston.kappa, heston.theta, heston.sigma, heston.rho, lambda, mu_j, sigma_j};
+    const int64_t off[2] = {0, 1};
+    double price = 0.0, grad[8];
+    check(ope_price_gradient_surfaces(OPE_MODEL_BATES, &c, 1, off, 1, p, &price, grad, nullptr));
+    return BatesJumpSensitivities{price, grad[5], grad[6], grad[7]};
+}
+
 struct MultistartResult {  // calibration.rs:70-76
     CalibResult best;
     size_t n_restarts, n_converged, n_pruned;

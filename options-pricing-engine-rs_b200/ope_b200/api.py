@@ -201,6 +201,24 @@ def bates_greeks_ad(spot, strike, expiry, rate, div_yield, heston, lam, mu_j, si
     return batch_greeks_ad(MODEL_BATES, c, np.concatenate([hp, [lam, mu_j, sigma_j]]), tol)[0]
 
 
+def heston_greeks_ad5(spot, strike, expiry, rate, div_yield, params, opt_type=OptionType.Call, tol=REF_TOL):
+    """ad.rs heston_greeks_ad5: the reference's joint five-parameter pass returns the
+    same PricingResult as heston_greeks_ad (ad.rs:1295-1322 checks exactly that),
+    so it maps to the same device computation."""
+    return heston_greeks_ad(spot, strike, expiry, rate, div_yield, params, opt_type, tol)
+
+
+def bates_jump_sensitivities_ad(spot, strike, expiry, rate, div_yield, heston, lam, mu_j, sigma_j,
+                                opt_type=OptionType.Call, tol=REF_TOL):
+    """ad.rs:882-895 (one contract): (price, d_lambda, d_mu_j, d_sigma_j) from the
+    reverse-mode adjoint."""
+    c = [OptionContract(spot, strike, expiry, rate, div_yield, 0.0, OptionType(opt_type))]
+    hp = _params_array(heston, MODEL_HESTON)
+    p = np.concatenate([hp, [lam, mu_j, sigma_j]])[None, :]
+    price, grad = price_gradient_surfaces(MODEL_BATES, c, [0, 1], p, tol)
+    return float(price[0]), float(grad[0, 5]), float(grad[0, 6]), float(grad[0, 7])
+
+
 def price_surfaces(model: int, contracts, surf_offsets, params, tol=REF_TOL, out=None,
                    bisections=None) -> np.ndarray:
     """Many surfaces (one parameter set each) in ONE persistent launch.
@@ -521,6 +539,7 @@ __all__ = [
     "price_surfaces", "price_surfaces_device", "batch_price_device", "contracts_array", "REF_TOL",
     "MODEL_HESTON", "MODEL_BATES", "RESULT_DTYPE", "kernel_launch_count", "device_info", "measure_fp64_peak", "price_gradient_surfaces",
     "price_gradient_surfaces_device", "batch_greeks_ad", "heston_greeks_ad", "bates_greeks_ad",
+    "heston_greeks_ad5", "bates_jump_sensitivities_ad",
     "CALIB_RESULT_DTYPE", "batch_implied_vol", "calibrate_surfaces", "calibrate_heston", "calibrate_bates", "calib_jacobian",
     "MULTISTART_RESULT_DTYPE", "GLOBAL_RESULT_DTYPE", "calibrate_surfaces_reg", "calibrate_multistart",
     "calibrate_global", "calibrate_heston_regularized", "calibrate_bates_regularized", "calibrate_heston_multistart",

@@ -105,3 +105,16 @@ def test_greeks_ad_empty_and_device_pointers(ope, oracle):
     torch.cuda.synchronize()
     dev = d_out.cpu().numpy().reshape(-1, 8)
     assert np.array_equal(dev, np.stack([host[nm] for nm in NAMES], axis=1))
+
+
+def test_aliases_of_the_reference_api(ope, oracle):  # ad.rs:1295-1322, 882-895
+    a = ope.heston_greeks_ad5(100.0, 100.0, 1.0, 0.05, 0.0, P, 0)
+    b = ope.heston_greeks_ad(100.0, 100.0, 1.0, 0.05, 0.0, P, 0)
+    assert a.tobytes() == b.tobytes()
+    price, dl, dm, ds = ope.bates_jump_sensitivities_ad(100.0, 100.0, 1.0, 0.05, 0.0, P, 0.5, -0.1, 0.15, 0)
+    c = oracle.contracts(100.0, 100.0, 1.0, 0.05, 0.0, 0)
+    rp, rg = oracle.price_gradient(c, P + JUMPS, True)
+    assert abs(price - rp) <= PRICE_TOL
+    for got, ref in zip((dl, dm, ds), rg[5:8]):
+        assert abs(got - ref) <= 1e-7 * abs(ref) + 1e-9 * S
+    assert dm < 0.0  # ad.rs:1022-1027
