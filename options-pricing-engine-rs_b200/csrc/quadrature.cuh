@@ -156,11 +156,13 @@ __device__ __forceinline__ double gk_integrate_warp(const CfConsts& C, double to
         }
         __syncwarp();
         if (!(err > tol && len < kMaxPanels)) break;
-        // argmax over the live list, last maximum wins (Iterator::max_by).
+        // argmax over the live list, last maximum wins (Iterator::max_by);
+        // chunks of 32 entries, stopping (warp-uniformly) after the last one in use
         unsigned long long best = 0ull;
         int bi = -1;
 #pragma unroll
         for (int j = 0; j < (kMaxPanels + 31) / 32; ++j) {
+            if (32 * j >= len) break;
             const int i = lane + 32 * j;
             if (i < len) {
                 const unsigned long long kk = L.ekey[i];
