@@ -514,7 +514,8 @@ def run_ours(args) -> None:
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": config_of(w, world),
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "api": "ope_price_surfaces (host pointers, pinned)"},
+                "api": "ope_price_surfaces (host pointers, pinned: the kernel reads the contracts and writes the prices "
+                       "in place over PCIe, zero-copy)"},
         "plain": {"value": plain_value, "unit": UNIT, "surfaces_sampled": int(picks.size),
                   "api": "ope_batch_bates per surface (host pointers, synchronous)",
                   "batched_e2e_over_plain": e2e_value / plain_value,

@@ -10,6 +10,10 @@
 
 #include "internal.h"
 
+#ifndef OPE_ZERO_COPY
+#define OPE_ZERO_COPY 1
+#endif
+
 namespace ope {
 
 ThreadCtx& tctx() {
@@ -112,6 +116,21 @@ int check_model(int32_t model) {
 bool device_ptrs(const ope_options* o) { return o && (o->flags & OPE_FLAG_DEVICE_PTRS); }
 cudaStream_t user_stream(const ope_options* o) { return o ? static_cast<cudaStream_t>(o->stream) : nullptr; }
 
+// Device address of a pinned (page-locked, mapped) host buffer, or nullptr
+// for pageable memory.  The pricing kernel reads each contract once and
+// writes each price once, so from pinned host buffers it works in place over
+// PCIe (zero-copy): the transfer overlaps the compute instead of preceding
+// and following it.
+void* pinned_device_ptr(const void* host) {
+    if (!OPE_ZERO_COPY) return nullptr;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, host) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return a.type == cudaMemoryTypeHost ? a.devicePointer : nullptr;
+}
+
 // Plain (one parameter set) pricing, host or device pointers.
 int batch_price(int32_t model, const ope_contract* contracts, size_t n, const void* params, double* out,
                 const ope_options* opts) {
@@ -137,11 +156,17 @@ int batch_price(int32_t model, const ope_contract* contracts, size_t n, const vo
     double* d_par = reinterpret_cast<double*>(p + b_con);
     double* d_out = reinterpret_cast<double*>(p + b_con + b_par);
     void* scratch = p + b_con + b_par + b_out;
-    OPE_CHECK(cudaMemcpyAsync(d_con, contracts, n * sizeof(ope_contract), cudaMemcpyHostToDevice, c.stream));
+    // contracts and prices in pinned host memory are used in place (zero-copy)
+    const ope_contract* k_con = static_cast<const ope_contract*>(pinned_device_ptr(contracts));
+    double* k_out = static_cast<double*>(pinned_device_ptr(out));
+    if (!k_con) {
+        OPE_CHECK(cudaMemcpyAsync(d_con, contracts, n * sizeof(ope_contract), cudaMemcpyHostToDevice, c.stream));
+        k_con = d_con;
+    }
     OPE_CHECK(cudaMemcpyAsync(d_par, params, stride * sizeof(double), cudaMemcpyHostToDevice, c.stream));
-    OPE_TRY(launch_price_persistent(model, d_con, n, nullptr, 1, nullptr, d_par, tol, d_out,
+    OPE_TRY(launch_price_persistent(model, k_con, n, nullptr, 1, nullptr, d_par, tol, k_out ? k_out : d_out,
                                     carve_price_scratch(scratch, n), c.stream));
-    OPE_CHECK(cudaMemcpyAsync(out, d_out, n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    if (!k_out) OPE_CHECK(cudaMemcpyAsync(out, d_out, n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
     OPE_CHECK(cudaStreamSynchronize(c.stream));
     return OPE_OK;
 }
@@ -461,12 +486,19 @@ int ope_price_surfaces_stats(int32_t model, const ope_contract* contracts, size_
     double* d_out = reinterpret_cast<double*>(p + b_con + b_off + b_par);
     int32_t* d_nb = out_bisections ? reinterpret_cast<int32_t*>(p + b_con + b_off + b_par + b_out) : nullptr;
     void* scratch = p + b_con + b_off + b_par + b_out + b_nb;
-    OPE_CHECK(cudaMemcpyAsync(d_con, contracts, n * sizeof(ope_contract), cudaMemcpyHostToDevice, c.stream));
+    // contracts and prices in pinned host memory are used in place (zero-copy)
+    const ope_contract* k_con = static_cast<const ope_contract*>(pinned_device_ptr(contracts));
+    double* k_out = static_cast<double*>(pinned_device_ptr(out_prices));
+    if (!k_con) {
+        OPE_CHECK(cudaMemcpyAsync(d_con, contracts, n * sizeof(ope_contract), cudaMemcpyHostToDevice, c.stream));
+        k_con = d_con;
+    }
     OPE_CHECK(cudaMemcpyAsync(d_off, surf_offsets, (n_surf + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, c.stream));
     OPE_CHECK(cudaMemcpyAsync(d_par, params, n_surf * stride * sizeof(double), cudaMemcpyHostToDevice, c.stream));
-    OPE_TRY(launch_price_persistent(model, d_con, n, d_off, n_surf, nullptr, d_par, tol, d_out,
+    OPE_TRY(launch_price_persistent(model, k_con, n, d_off, n_surf, nullptr, d_par, tol, k_out ? k_out : d_out,
                                     carve_price_scratch(scratch, n), c.stream, d_nb));
-    OPE_CHECK(cudaMemcpyAsync(out_prices, d_out, n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    if (!k_out)
+        OPE_CHECK(cudaMemcpyAsync(out_prices, d_out, n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
     if (out_bisections)
         OPE_CHECK(cudaMemcpyAsync(out_bisections, d_nb, 2 * n * sizeof(int32_t), cudaMemcpyDeviceToHost, c.stream));
     OPE_CHECK(cudaStreamSynchronize(c.stream));

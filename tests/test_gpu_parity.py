@@ -285,3 +285,22 @@ def test_newton_reciprocal_and_sqrt_within_two_ulp(ope):
     a, b = ctypes.c_uint64(), ctypes.c_uint64()
     _lib.check(_lib.load().ope_selftest_math(ctypes.byref(a), ctypes.byref(b)))
     assert a.value <= 2 and b.value <= 2, (a.value, b.value)
+
+
+def test_pinned_host_buffers_zero_copy_equal_copy_path(ope):
+    """Contracts and prices in pinned host memory are read and written in place
+    by the kernel (zero-copy); the prices equal the pageable (copy) path's."""
+    import torch
+
+    w = W.c3(n=1 << 14, per_surface=256, seed=17)
+    pin_con = torch.empty(w.n * 56, dtype=torch.uint8, pin_memory=True).numpy().view(w.contracts.dtype)
+    pin_con[:] = w.contracts
+    pin_out = torch.empty(w.n, dtype=torch.float64, pin_memory=True).numpy()
+    pin_out[:] = np.nan
+    ope.price_surfaces(ope.MODEL_BATES, pin_con, w.surf_offsets, w.params, tol=w.tol, out=pin_out)
+    ref = ope.price_surfaces(ope.MODEL_BATES, w.contracts, w.surf_offsets, w.params, tol=w.tol)
+    assert np.array_equal(pin_out, ref)
+    # the plain one-parameter-set call, pinned contracts and pageable output
+    sub = pin_con[:256]
+    got = ope.batch_bates(sub, w.params[0], tol=w.tol)
+    assert np.array_equal(got, ref[:256])
