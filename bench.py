@@ -377,6 +377,15 @@ def bench_serving(args) -> dict:
     return out
 
 
+def nodes_percentiles(nb) -> dict:
+    """Integrand evaluations per contract (both integrals: 15 (1 + 2 bisections)
+    each) as percentiles over the batch; the load imbalance the work queue absorbs."""
+    nodes = 15 * (1 + 2 * nb.reshape(-1, 2).astype(np.int64)).sum(axis=1)
+    return {"p50": float(np.percentile(nodes, 50)), "p90": float(np.percentile(nodes, 90)),
+            "p99": float(np.percentile(nodes, 99)), "max": int(nodes.max()),
+            "integrals_at_panel_cap": int((nb >= 199).sum())}
+
+
 def read_traffic():
     p = os.path.join(ROOT, "profiles", "c3_persistent_traffic.json")
     if os.path.exists(p):
@@ -527,7 +536,8 @@ def run_ours(args) -> None:
                      "work": f"{flops_per_launch:.4e} FP64 ops per launch = nodes x F_node "
                              f"(F_node {roofline.F_NODE[(True, True)]}/{roofline.F_NODE[(True, False)]} P1/P2); "
                              f"nodes/contract {roofline.nodes_total(nb) / n:.1f}",
-                     "kernel_ms": kern_avg},
+                     "kernel_ms": kern_avg,
+                     "nodes_per_contract": nodes_percentiles(nb)},
         "gpu_launches": int(launches),
         "clocks": clk,
     }

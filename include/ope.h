@@ -115,6 +115,15 @@ int ope_device_info(int32_t* sm_count, int32_t* cc_major, int32_t* cc_minor);
 /* Device kernels launched by this library on the calling thread since load. */
 uint64_t ope_kernel_launch_count(void);
 
+/* No reference counterpart.  Caps the device workspace the calling thread's
+ * calls may hold (bytes; 0 = no cap).  A call that needs more fails with
+ * OPE_ERR_OUT_OF_MEMORY before allocating anything; a workspace already held
+ * above the new cap is freed.  The request server's slab and the
+ * allocation-free entry point are not affected. */
+int ope_set_workspace_limit(uint64_t bytes);
+/* Bytes of device workspace the calling thread holds. */
+uint64_t ope_workspace_bytes(void);
+
 /* ------------------------------------------------ reference drop-ins */
 /* heston.rs:61-72 heston_price.  One contract. */
 int ope_heston_price(double spot, double strike, double expiry, double rate, double div_yield,

@@ -65,6 +65,10 @@ int ensure_device() {
 
 int ensure_workspace(size_t bytes, void** out) {
     ThreadCtx& c = tctx();
+    if (c.ws_limit && bytes > c.ws_limit)
+        return set_error(OPE_ERR_OUT_OF_MEMORY, "call needs " + std::to_string(bytes) +
+                                                    " bytes of device workspace, above this thread's limit of " +
+                                                    std::to_string(c.ws_limit) + " (ope_set_workspace_limit)");
     if (bytes > c.ws_bytes) {
         if (c.ws) {
             OPE_CHECK(cudaDeviceSynchronize());
@@ -74,6 +78,7 @@ int ensure_workspace(size_t bytes, void** out) {
         }
         size_t want = std::max(bytes, c.ws_bytes + c.ws_bytes / 2);
         want = align_up(want, 1 << 20);
+        if (c.ws_limit) want = std::max(bytes, std::min(want, c.ws_limit));
         OPE_CHECK(cudaMalloc(&c.ws, want));
         c.ws_bytes = want;
     }
@@ -134,6 +139,7 @@ void* pinned_device_ptr(const void* host) {
 // Plain (one parameter set) pricing, host or device pointers.
 int batch_price(int32_t model, const ope_contract* contracts, size_t n, const void* params, double* out,
                 const ope_options* opts) {
+    OPE_RANGE("ope.batch_price");
     OPE_TRY(check_model(model));
     double tol;
     OPE_TRY(resolve_tol(opts, &tol));
@@ -173,6 +179,7 @@ int batch_price(int32_t model, const ope_contract* contracts, size_t n, const vo
 
 int batch_greeks(int32_t model, const ope_contract* contracts, size_t n, const void* params,
                  ope_pricing_result* out, const ope_options* opts, bool ad = false) {
+    OPE_RANGE(ad ? "ope.batch_greeks_ad" : "ope.batch_greeks");
     OPE_TRY(check_model(model));
     double tol;
     OPE_TRY(resolve_tol(opts, &tol));
@@ -219,6 +226,20 @@ const char* ope_last_error(void) { return tctx().last_error.c_str(); }
 const char* ope_version(void) { return "ope-b200 0.1.0 (sm_100a, FP64 greedy GK15)"; }
 
 uint64_t ope_kernel_launch_count(void) { return tctx().launches; }
+
+int ope_set_workspace_limit(uint64_t bytes) {
+    ThreadCtx& c = tctx();
+    c.ws_limit = (size_t)bytes;
+    if (bytes && c.ws && c.ws_bytes > bytes) {  // give back a workspace above the new cap
+        OPE_CHECK(cudaDeviceSynchronize());
+        OPE_CHECK(cudaFree(c.ws));
+        c.ws = nullptr;
+        c.ws_bytes = 0;
+    }
+    return OPE_OK;
+}
+
+uint64_t ope_workspace_bytes(void) { return tctx().ws_bytes; }
 
 int ope_device_info(int32_t* sm_count, int32_t* cc_major, int32_t* cc_minor) {
     OPE_TRY(ensure_device());
@@ -279,6 +300,7 @@ int ope_batch_greeks_ad(int32_t model, const ope_contract* contracts, size_t n, 
 
 int ope_batch_implied_vol(const ope_contract* contracts, size_t n, const double* market_prices, double* out_iv,
                           int32_t* out_ok, const ope_options* opts) {
+    OPE_RANGE("ope.batch_implied_vol");
     if (n == 0) return OPE_OK;
     if (!contracts || !market_prices || !out_iv || !out_ok) return set_error(OPE_ERR_INVALID_ARG, "NULL argument");
     OPE_TRY(ensure_device());
@@ -305,6 +327,7 @@ int ope_batch_implied_vol(const ope_contract* contracts, size_t n, const double*
 int ope_calibrate_surfaces(int32_t model, const ope_contract* quotes, const double* iv_market, const double* weights,
                            size_t n_quotes, const int64_t* surf_offsets, size_t n_surf, const double* p0,
                            ope_calib_result* out, const ope_options* opts) {
+    OPE_RANGE("ope.calibrate_surfaces");
     OPE_TRY(check_model(model));
     double tol;
     OPE_TRY(resolve_tol(opts, &tol));
@@ -320,6 +343,7 @@ int ope_calibrate_surfaces_reg(int32_t model, const ope_contract* quotes, const 
                                const double* weights, size_t n_quotes, const int64_t* surf_offsets, size_t n_surf,
                                const double* p0, const double* prior, const double* reg_weight,
                                ope_calib_result* out, const ope_options* opts) {
+    OPE_RANGE("ope.calibrate_surfaces_reg");
     OPE_TRY(check_model(model));
     double tol;
     OPE_TRY(resolve_tol(opts, &tol));
@@ -341,6 +365,7 @@ int ope_calibrate_multistart(int32_t model, const ope_contract* quotes, const do
                              const double* weights, size_t n_quotes, const int64_t* surf_offsets, size_t n_surf,
                              const double* p0, int32_t n_restarts, uint64_t seed, const double* shared_best0,
                              ope_multistart_result* out, ope_calib_result* out_restarts, const ope_options* opts) {
+    OPE_RANGE("ope.calibrate_multistart");
     OPE_TRY(check_model(model));
     double tol;
     OPE_TRY(resolve_tol(opts, &tol));
@@ -357,6 +382,7 @@ int ope_calibrate_global(int32_t model, const ope_contract* quotes, const double
                          size_t n_quotes, const int64_t* surf_offsets, size_t n_surf, int32_t n_pop, int32_t n_gen,
                          uint64_t seed, const double* prior, const double* reg_weight, ope_global_result* out,
                          const ope_options* opts) {
+    OPE_RANGE("ope.calibrate_global");
     OPE_TRY(check_model(model));
     double tol;
     OPE_TRY(resolve_tol(opts, &tol));
@@ -375,6 +401,7 @@ int ope_calibrate_global(int32_t model, const ope_contract* quotes, const double
 int ope_calib_jacobian(int32_t model, const ope_contract* quotes, const double* iv_market, size_t n_quotes,
                        const int64_t* surf_offsets, size_t n_surf, const double* params, double* out_jac,
                        double* out_res, const ope_options* opts) {
+    OPE_RANGE("ope.calib_jacobian");
     OPE_TRY(check_model(model));
     double tol;
     OPE_TRY(resolve_tol(opts, &tol));
@@ -391,6 +418,7 @@ int ope_calib_jacobian(int32_t model, const ope_contract* quotes, const double* 
 int ope_price_gradient_surfaces(int32_t model, const ope_contract* contracts, size_t n, const int64_t* surf_offsets,
                                 size_t n_surf, const void* params, double* out_prices, double* out_grad,
                                 const ope_options* opts) {
+    OPE_RANGE("ope.price_gradient_surfaces");
     OPE_TRY(check_model(model));
     double tol;
     OPE_TRY(resolve_tol(opts, &tol));
@@ -453,6 +481,7 @@ int ope_price_surfaces(int32_t model, const ope_contract* contracts, size_t n, c
 int ope_price_surfaces_stats(int32_t model, const ope_contract* contracts, size_t n, const int64_t* surf_offsets,
                              size_t n_surf, const void* params, double* out_prices, int32_t* out_bisections,
                              const ope_options* opts) {
+    OPE_RANGE("ope.price_surfaces");
     OPE_TRY(check_model(model));
     double tol;
     OPE_TRY(resolve_tol(opts, &tol));

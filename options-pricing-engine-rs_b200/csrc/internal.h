@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <stddef.h>
 #include <stdint.h>
 
@@ -26,6 +27,7 @@ struct ThreadCtx {
     size_t pinned_bytes = 0;
     std::string last_error;
     uint64_t launches = 0;
+    size_t ws_limit = 0;         // cap on the device workspace (0: none), ope_set_workspace_limit
     double grid_fraction = 1.0;  // persistent launches fill at most this share of the block slots
 };
 
@@ -35,6 +37,16 @@ int check_cuda(cudaError_t e, const char* what);
 int ensure_device();                               // OPE_OK or OPE_ERR_NO_DEVICE
 int ensure_workspace(size_t bytes, void** out);    // grows the per-thread workspace
 int ensure_pinned(size_t bytes, void** out);       // grows the pinned staging buffer
+
+// Profiler ranges (NVTX, header-only: free when no tool is attached), one
+// per C-ABI call and per server micro-batch.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
+#define OPE_RANGE(name) ::ope::NvtxRange _ope_nvtx_range(name)
 
 #define OPE_CHECK(call)                                        \
     do {                                                       \

@@ -258,6 +258,7 @@ bool launch_batch(Server& S, int kind, std::unique_lock<std::mutex>& lk) {
     // The requests, slot, device and pinned regions now belong to this batch:
     // pack and enqueue without the lock.
     lk.unlock();
+    OPE_RANGE(kind == RK_PRICE ? "ope.server.reprice_batch" : "ope.server.calibration_batch");
     char* p = pin;
     ope_contract* con_h = reinterpret_cast<ope_contract*>(p);
     p += align_up(n * sizeof(ope_contract), 256);

@@ -58,6 +58,8 @@ _vp, _d, _i32, _sz, _u64 = ctypes.c_void_p, ctypes.c_double, ctypes.c_int32, cty
 _sig("ope_last_error", ctypes.c_char_p, [])
 _sig("ope_version", ctypes.c_char_p, [])
 _sig("ope_kernel_launch_count", _u64, [])
+_sig("ope_set_workspace_limit", ctypes.c_int, [_u64])
+_sig("ope_workspace_bytes", _u64, [])
 _sig("ope_device_info", ctypes.c_int, [ctypes.POINTER(_i32)] * 3)
 _sig("ope_heston_price", ctypes.c_int, [_d, _d, _d, _d, _d, _vp, _i32, ctypes.POINTER(_d)])
 _sig("ope_bates_price", ctypes.c_int, [_d, _d, _d, _d, _d, _vp, _i32, ctypes.POINTER(_d)])

@@ -523,6 +523,17 @@ def batch_price_device(model: int, d_contracts, n: int, d_params, d_out, tol=REF
     check(load().ope_batch_price_ex(model, ptr(d_contracts), n, ptr(d_params), ptr(d_out), ctypes.byref(o)))
 
 
+def set_workspace_limit(nbytes: int) -> None:
+    """Cap the device workspace of the calling thread's calls (0: no cap); a call
+    needing more raises OpeError(OPE_ERR_OUT_OF_MEMORY) before allocating."""
+    check(load().ope_set_workspace_limit(int(nbytes)))
+
+
+def workspace_bytes() -> int:
+    """Device workspace bytes the calling thread holds."""
+    return int(load().ope_workspace_bytes())
+
+
 def kernel_launch_count() -> int:
     return int(load().ope_kernel_launch_count())
 
@@ -539,7 +550,7 @@ __all__ = [
     "price_surfaces", "price_surfaces_device", "batch_price_device", "contracts_array", "REF_TOL",
     "MODEL_HESTON", "MODEL_BATES", "RESULT_DTYPE", "kernel_launch_count", "device_info", "measure_fp64_peak", "price_gradient_surfaces",
     "price_gradient_surfaces_device", "batch_greeks_ad", "heston_greeks_ad", "bates_greeks_ad",
-    "heston_greeks_ad5", "bates_jump_sensitivities_ad",
+    "heston_greeks_ad5", "bates_jump_sensitivities_ad", "set_workspace_limit", "workspace_bytes",
     "CALIB_RESULT_DTYPE", "batch_implied_vol", "calibrate_surfaces", "calibrate_heston", "calibrate_bates", "calib_jacobian",
     "MULTISTART_RESULT_DTYPE", "GLOBAL_RESULT_DTYPE", "calibrate_surfaces_reg", "calibrate_multistart",
     "calibrate_global", "calibrate_heston_regularized", "calibrate_bates_regularized", "calibrate_heston_multistart",

@@ -58,3 +58,9 @@ def test_api_rejects_wrong_param_shapes(ope):
     with pytest.raises(ValueError):
         ope.price_surfaces(ope.MODEL_HESTON, np.zeros(2, ope.api.CONTRACT_DTYPE), [0, 1, 2],
                            [[0.04, 2.0, 0.04, 0.3, -0.7]])
+
+
+def test_workspace_limit_needs_no_device(ope):
+    ope.set_workspace_limit(1 << 20)
+    ope.set_workspace_limit(0)
+    assert ope.workspace_bytes() == 0

@@ -304,3 +304,24 @@ def test_pinned_host_buffers_zero_copy_equal_copy_path(ope):
     sub = pin_con[:256]
     got = ope.batch_bates(sub, w.params[0], tol=w.tol)
     assert np.array_equal(got, ref[:256])
+
+
+def test_workspace_limit_fails_cleanly_and_recovers(ope):
+    """Injected allocation failure without a GPU fault: under a 1 MiB workspace
+    cap a call that needs more fails with OPE_ERR_OUT_OF_MEMORY before
+    allocating anything; small calls still run; lifting the cap restores
+    normal operation with unchanged results."""
+    w = W.c3(n=1 << 14, per_surface=256, seed=23)
+    ref = ope.price_surfaces(ope.MODEL_BATES, w.contracts, w.surf_offsets, w.params, tol=w.tol)
+    try:
+        ope.set_workspace_limit(1 << 20)
+        assert ope.workspace_bytes() <= 1 << 20
+        with pytest.raises(ope.OpeError) as e:
+            ope.price_surfaces(ope.MODEL_BATES, w.contracts, w.surf_offsets, w.params, tol=w.tol)
+        assert e.value.status == 2 and "limit" in str(e.value)
+        small = ope.batch_bates(w.contracts[:64], w.params[0], tol=w.tol)
+        assert np.array_equal(small, ref[:64])
+    finally:
+        ope.set_workspace_limit(0)
+    again = ope.price_surfaces(ope.MODEL_BATES, w.contracts, w.surf_offsets, w.params, tol=w.tol)
+    assert np.array_equal(again, ref)
