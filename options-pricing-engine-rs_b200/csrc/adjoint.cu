@@ -89,8 +89,11 @@ __global__ void __launch_bounds__(128, OPE_GRAD_MINB) k_grad_backward(const ope_
         const CfConsts C = make_consts(__ldg(&cp->spot), __ldg(&cp->strike), __ldg(&cp->expiry), __ldg(&cp->rate),
                                        pl, BATES, which);
         const GradParams G = make_grad_params(pl, BATES);
-        const size_t pidx = (size_t)unit * src.n_slots + (src.slot ? __ldg(src.slot + s) : 0);
-        const int len = __ldg(src.nbis + pidx) + 1;
+        int slot = src.slot ? __ldg(src.slot + s) : 0;
+        if (!ope_check(slot >= 0 && slot < src.n_slots, CHK_SLOT)) slot = 0;
+        const size_t pidx = (size_t)unit * src.n_slots + slot;
+        int len = __ldg(src.nbis + pidx) + 1;
+        if (!ope_check(len >= 1 && len <= kMaxPanels, CHK_PANEL_LEN)) len = len < 1 ? 1 : kMaxPanels;
         const double* P = src.panels + pidx * (2 * kMaxPanels);
         double acc[DIM];
 #pragma unroll

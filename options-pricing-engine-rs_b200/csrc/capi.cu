@@ -8,6 +8,7 @@
 #include <cstring>
 #include <string>
 
+#include "checked.cuh"
 #include "internal.h"
 
 #ifndef OPE_ZERO_COPY
@@ -15,6 +16,10 @@
 #endif
 
 namespace ope {
+
+#if OPE_CHECKED
+__device__ unsigned int g_ope_check_word = 0;
+#endif
 
 ThreadCtx& tctx() {
     static thread_local ThreadCtx c;
@@ -226,6 +231,21 @@ const char* ope_last_error(void) { return tctx().last_error.c_str(); }
 const char* ope_version(void) { return "ope-b200 0.1.0 (sm_100a, FP64 greedy GK15)"; }
 
 uint64_t ope_kernel_launch_count(void) { return tctx().launches; }
+
+int ope_check_word(uint32_t* out_word, int32_t* out_checked_build) {
+    if (!out_word) return set_error(OPE_ERR_INVALID_ARG, "NULL argument");
+    *out_word = 0;
+    if (out_checked_build) *out_checked_build = OPE_CHECKED;
+#if OPE_CHECKED
+    OPE_TRY(ensure_device());
+    unsigned int w = 0;
+    OPE_CHECK(cudaMemcpyFromSymbol(&w, g_ope_check_word, sizeof(w)));
+    const unsigned int zero = 0;
+    OPE_CHECK(cudaMemcpyToSymbol(g_ope_check_word, &zero, sizeof(zero)));
+    *out_word = w;
+#endif
+    return OPE_OK;
+}
 
 int ope_set_workspace_limit(uint64_t bytes) {
     ThreadCtx& c = tctx();

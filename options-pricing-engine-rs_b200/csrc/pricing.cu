@@ -158,7 +158,9 @@ __global__ void __launch_bounds__(OPE_KERNEL_WARPS * 32, OPE_KERNEL_MINB) k_pric
                 atomicMax(head, 2ull * (unsigned long long)__ldg(surf_off + s + 1));
             continue;
         }
-        const int slot = (SAVE && sink.slot) ? __ldg(sink.slot + s) : 0;
+        if (!param_idx && n_surf > 1 && !ope_check(s >= 0 && s < n_surf, CHK_SURFACE)) continue;
+        int slot = (SAVE && sink.slot) ? __ldg(sink.slot + s) : 0;
+        if (SAVE && !ope_check(slot >= 0 && slot < sink.n_slots, CHK_SLOT)) slot = 0;
         run_unit<BATES, SAVE>(c, (int)(unit & 1), con, params + s * stride, tol, out, integ, done, nbis_out,
                               sink, slot, smem_panels[warp], lane, R);
     }

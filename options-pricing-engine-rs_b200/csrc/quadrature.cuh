@@ -22,6 +22,7 @@
 #pragma once
 
 #include "cf_device.cuh"
+#include "checked.cuh"
 
 namespace ope {
 
@@ -156,6 +157,7 @@ __device__ __forceinline__ double gk_integrate_warp(const CfConsts& C, double to
         }
         __syncwarp();
         if (!(err > tol && len < kMaxPanels)) break;
+        if (!ope_check(len < kMaxPanels, CHK_PANEL_COUNT)) break;
         // argmax over the live list, last maximum wins (Iterator::max_by);
         // chunks of 32 entries, stopping (warp-uniformly) after the last one in use
         unsigned long long best = 0ull;
@@ -175,6 +177,7 @@ __device__ __forceinline__ double gk_integrate_warp(const CfConsts& C, double to
             const int oi = __shfl_xor_sync(FULL, bi, off);
             if (ob > best || (ob == best && oi > bi)) { best = ob; bi = oi; }
         }
+        if (!ope_check(bi >= 0 && bi < len, CHK_PANEL_INDEX)) bi = 0;
         w = bi;
         ew = __longlong_as_double((long long)best);
         kw = L.k[w];

@@ -60,6 +60,7 @@ _sig("ope_version", ctypes.c_char_p, [])
 _sig("ope_kernel_launch_count", _u64, [])
 _sig("ope_set_workspace_limit", ctypes.c_int, [_u64])
 _sig("ope_workspace_bytes", _u64, [])
+_sig("ope_check_word", ctypes.c_int, [ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(_i32)])
 _sig("ope_device_info", ctypes.c_int, [ctypes.POINTER(_i32)] * 3)
 _sig("ope_heston_price", ctypes.c_int, [_d, _d, _d, _d, _d, _vp, _i32, ctypes.POINTER(_d)])
 _sig("ope_bates_price", ctypes.c_int, [_d, _d, _d, _d, _d, _vp, _i32, ctypes.POINTER(_d)])
@@ -98,6 +99,22 @@ _sig("ope_price_surfaces_noalloc", ctypes.c_int, [_i32, _vp, _sz, _vp, _sz, _vp,
 _sig("ope_measure_fp64_peak", ctypes.c_int, [ctypes.POINTER(_d), ctypes.POINTER(_d)])
 
 _lib = None
+
+
+CHECKED_LIB_PATH = os.path.join(PKG_ROOT, "lib", "checked", "libope_b200.so")
+
+
+def open_library(path: str) -> ctypes.CDLL:
+    """A separate handle on a build of the library at `path` (e.g. the
+    bounds-checked build), with the ABI signatures applied."""
+    L = ctypes.CDLL(path)
+    for name, (res, args) in _SIGS.items():
+        fn = getattr(L, name, None)
+        if fn is None:
+            continue
+        fn.restype = res
+        fn.argtypes = args
+    return L
 
 
 def load() -> ctypes.CDLL:
