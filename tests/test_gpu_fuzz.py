@@ -1,0 +1,49 @@
+"""GPU: randomised parity against the oracle over wider ranges than the
+benchmark configurations -- vol-of-vol up to 3, correlation up to +-0.99,
+mean reversion from 0.05 to 20, Feller violated half the time, expiries from
+one day to ten years, strikes from deep in to deep out of the money, jump
+intensities up to 5 -- at the reference's tolerance and at 1e-10, one
+parameter set per contract.  The bar is the parity bar: 1e-9 S per contract.
+Where the reference's own formula gives a non-finite price the device must
+too (checked by comparing the finite masks)."""
+import numpy as np
+import pytest
+
+from ope_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+S = 100.0
+
+
+def _draw(rng, n, bates):
+    con = np.zeros(n, W.CONTRACT_DTYPE)
+    t = np.exp(rng.uniform(np.log(1 / 365), np.log(10.0), n))
+    r = rng.uniform(-0.01, 0.08, n)
+    q = rng.uniform(0.0, 0.05, n)
+    m = rng.uniform(-2.0, 1.2, n) * np.sqrt(np.minimum(t, 1.0))
+    con["spot"], con["strike"], con["expiry"] = S, S * np.exp((r - q) * t + m), t
+    con["rate"], con["div_yield"], con["vol"] = r, q, 0.2
+    con["opt_type"] = rng.integers(0, 2, n)
+    p = np.column_stack([rng.uniform(0.005, 0.6, n), np.exp(rng.uniform(np.log(0.05), np.log(20.0), n)),
+                         rng.uniform(0.005, 0.6, n), rng.uniform(0.05, 3.0, n), rng.uniform(-0.99, 0.99, n)])
+    if bates:
+        p = np.column_stack([p, rng.uniform(0.0, 5.0, n), rng.uniform(-0.5, 0.3, n), rng.uniform(0.02, 0.6, n)])
+    return con, p
+
+
+@pytest.mark.parametrize("bates", [False, True])
+@pytest.mark.parametrize("tol", [1e-8, 1e-10])
+def test_wide_range_parity(ope, oracle, bates, tol):
+    rng = np.random.default_rng(2024 + 7 * bates + int(tol < 1e-9))
+    n = 8000
+    con, p = _draw(rng, n, bates)
+    off = np.arange(n + 1, dtype=np.int64)  # one parameter set (surface) per contract
+    got = ope.price_surfaces(ope.MODEL_BATES if bates else ope.MODEL_HESTON, con, off, p, tol=tol)
+    ref = oracle.batch_price(con, p, bates, tol, surf_idx=np.arange(n, dtype=np.int32))
+    fin = np.isfinite(ref)
+    assert np.array_equal(np.isfinite(got), fin)
+    err = np.abs(got[fin] - ref[fin])
+    worst = int(np.argmax(err))
+    print(f"bates={bates} tol={tol}: {fin.sum()} finite of {n}, worst |gpu - oracle| / S = {err.max() / S:.2e}")
+    assert err.max() <= 1e-9 * S, (float(err.max()), con[fin][worst], p[fin][worst])
