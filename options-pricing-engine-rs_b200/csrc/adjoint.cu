@@ -132,11 +132,16 @@ __global__ void __launch_bounds__(128, OPE_GRAD_MINB) k_grad_backward(const ope_
         sw_im = warp_sum(sw_im);
         if (which == 0) {
             // -d Log CF(-i)/dp, constant over the integral (zero up to rounding for a
-            // regular normaliser; ad.rs:705-706 carries it through the Dual division)
+            // regular normaliser; ad.rs:705-706 carries it through the Dual division).
+            // Where it is not finite (e.g. kappa < rho sigma puts xi + d = 0 at
+            // phi = -i), every P1 node's derivative is non-finite in the reference,
+            // so every node is dropped (ad.rs:679-682) and the component is 0.
             __syncwarp();
 #pragma unroll
-            for (int k = 0; k < DIM; ++k)
-                acc[k] -= (c2(s_norm[warp][2 * k], s_norm[warp][2 * k + 1]) * c2(sw_re, sw_im)).im;
+            for (int k = 0; k < DIM; ++k) {
+                const C2 dl = c2(s_norm[warp][2 * k], s_norm[warp][2 * k + 1]);
+                acc[k] = (isfinite(dl.re) && isfinite(dl.im)) ? acc[k] - (dl * c2(sw_re, sw_im)).im : 0.0;
+            }
             __syncwarp();
         }
         if (lane == 0) {

@@ -47,3 +47,23 @@ def test_wide_range_parity(ope, oracle, bates, tol):
     worst = int(np.argmax(err))
     print(f"bates={bates} tol={tol}: {fin.sum()} finite of {n}, worst |gpu - oracle| / S = {err.max() / S:.2e}")
     assert err.max() <= 1e-9 * S, (float(err.max()), con[fin][worst], p[fin][worst])
+
+
+@pytest.mark.parametrize("bates", [False, True])
+def test_wide_range_gradient_parity(ope, oracle, bates):
+    """The reverse-mode gradient against the oracle's forward-mode AD
+    (ad.rs:695-731, 882-895) over the same wide ranges, at the adjoint's bar:
+    1e-7 relative plus 1e-9 S absolute per component."""
+    rng = np.random.default_rng(77 + bates)
+    n = 2000
+    con, p = _draw(rng, n, bates)
+    off = np.arange(n + 1, dtype=np.int64)
+    price, grad = ope.price_gradient_surfaces(ope.MODEL_BATES if bates else ope.MODEL_HESTON, con, off, p, tol=1e-8)
+    rp, rg = oracle.batch_price_gradient(con, p, bates, 1e-8, surf_idx=np.arange(n, dtype=np.int32))
+    fin = np.all(np.isfinite(rg), axis=1) & np.isfinite(rp)
+    assert fin.mean() > 0.99
+    lim = 1e-7 * np.abs(rg[fin]) + 1e-9 * S
+    ratio = np.abs(grad[fin] - rg[fin]) / lim
+    i, k = np.unravel_index(int(np.argmax(ratio)), ratio.shape)
+    print(f"bates={bates}: {fin.sum()} of {n}, worst error / bar = {ratio.max():.3g} (component {k})")
+    assert ratio.max() <= 1.0, (float(ratio.max()), int(k), con[fin][i], p[fin][i], grad[fin][i], rg[fin][i])
