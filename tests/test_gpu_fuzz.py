@@ -67,3 +67,74 @@ def test_wide_range_gradient_parity(ope, oracle, bates):
     i, k = np.unravel_index(int(np.argmax(ratio)), ratio.shape)
     print(f"bates={bates}: {fin.sum()} of {n}, worst error / bar = {ratio.max():.3g} (component {k})")
     assert ratio.max() <= 1.0, (float(ratio.max()), int(k), con[fin][i], p[fin][i], grad[fin][i], rg[fin][i])
+
+
+NAMES = ["price", "delta", "gamma", "vega", "theta", "rho", "vanna", "volga"]
+# finite-difference amplification of the 1e-9 S price bar in each Greek's formula
+AMP = {"price": 1, "delta": 1, "gamma": 4, "vega": 100, "theta": 2 * 365, "rho": 1e4, "vanna": 200, "volga": 2e4}
+
+
+@pytest.mark.parametrize("bates", [False, True])
+def test_wide_range_bump_greeks(ope, oracle, bates):
+    """greeks.rs:19-72 (14 pricings per contract) over the wide ranges: 24
+    random parameter sets x 64 random contracts each, against the oracle."""
+    rng = np.random.default_rng(501 + bates)
+    worst = 0.0
+    for _ in range(24):
+        con, p = _draw(rng, 64, bates)
+        got = (ope.batch_bates_greeks if bates else ope.batch_heston_greeks)(con, p[0], tol=1e-10)
+        ref = oracle.batch_greeks(con, p[0], bates, tol=1e-10)
+        fin = np.all(np.isfinite(ref), axis=1)
+        for i, nm in enumerate(NAMES):
+            err = np.abs(got[nm][fin] - ref[fin, i]) / (1e-9 * S * AMP[nm])
+            worst = max(worst, float(err.max()))
+            assert err.max() <= 1.0, (nm, float(err.max()), p[0])
+    print(f"bates={bates}: bump Greeks worst error / bar = {worst:.3g}")
+
+
+@pytest.mark.parametrize("bates", [False, True])
+def test_wide_range_ad_greeks(ope, oracle, bates):
+    """ad.rs:736-865 over the wide ranges: 16 parameter sets x 32 contracts."""
+    rng = np.random.default_rng(601 + bates)
+    worst = 0.0
+    for _ in range(16):
+        con, p = _draw(rng, 32, bates)
+        got = ope.batch_greeks_ad(ope.MODEL_BATES if bates else ope.MODEL_HESTON, con, p[0], tol=1e-8)
+        ref = np.array([oracle.greeks_ad(c, p[0], bates, 1e-8) for c in con])
+        fin = np.all(np.isfinite(ref), axis=1)
+        for i, nm in enumerate(NAMES):
+            bar = 1e-9 * S * AMP[nm]
+            if nm == "vega":
+                bar = bar + 1e-7 * np.abs(ref[fin, 3])
+            if nm == "volga":
+                bar = bar + 1e-7 * 2.0 * (np.abs(ref[fin, 3]) + 1.0) / 0.02
+            err = np.abs(got[nm][fin] - ref[fin, i]) / bar
+            worst = max(worst, float(err.max()))
+            assert err.max() <= 1.0, (nm, float(err.max()), p[0])
+    print(f"bates={bates}: AD Greeks worst error / bar = {worst:.3g}")
+
+
+def test_wide_range_implied_vol(ope, oracle):
+    """iv.rs:14-95 on the device over BSM prices of random contracts (vol from
+    1 % to 300 %, expiries from a day to ten years), against the oracle: the
+    same ok flags where the price carries time value, and the same IVs at the
+    vega-scaled bar of the IV tests."""
+    rng = np.random.default_rng(701)
+    n = 20000
+    con, _ = _draw(rng, n, False)
+    con["vol"] = np.exp(rng.uniform(np.log(0.01), np.log(3.0), n))
+    px = np.array([oracle.bsm_price(c) for c in con])
+    got, ok = ope.batch_implied_vol(con, px)
+    ref, rok = oracle.batch_implied_vol(con, px)
+    eq, er = np.exp(-con["div_yield"] * con["expiry"]), np.exp(-con["rate"] * con["expiry"])
+    intrinsic = np.where(con["opt_type"] == 0, np.maximum(S * eq - con["strike"] * er, 0.0),
+                         np.maximum(con["strike"] * er - S * eq, 0.0))
+    ident = (px - intrinsic) > 1e-9 * S
+    assert np.array_equal(ok[ident].astype(bool), rok[ident].astype(bool))
+    both = ident & ok.astype(bool) & rok.astype(bool)
+    vega = np.array([oracle.bsm_price_and_greeks(oracle.contracts(c["spot"], c["strike"], c["expiry"], c["rate"],
+                                                                  c["div_yield"], c["opt_type"], vol=v))[3]
+                     for c, v in zip(con[both], ref[both])])
+    err = np.abs(got[both] - ref[both]) / (2.5e-10 / np.maximum(vega, 1e-300) + 1e-12)
+    print(f"implied vol: {both.sum()} of {n} compared, worst error / bar = {err.max():.3g}")
+    assert err.max() <= 1.0
