@@ -176,9 +176,7 @@ __global__ void k_grad_combine(const ope_contract* __restrict__ con, long long n
 template <class K>
 int grad_grid(K kernel, size_t smem, unsigned long long need, int* grid) {
     int per_sm = 0;
-    OPE_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    OPE_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 128, smem));
-    if (per_sm < 1) per_sm = 1;
+    OPE_TRY(blocks_per_sm(reinterpret_cast<const void*>(kernel), 128, smem, &per_sm));
     const int cap = std::max(1, (int)(per_sm * tctx().sm_count * tctx().grid_fraction));
     *grid = (int)std::min<unsigned long long>((unsigned long long)cap, need);
     return OPE_OK;

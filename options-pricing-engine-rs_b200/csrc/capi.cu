@@ -6,7 +6,10 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
+#include <tuple>
 
 #include "checked.cuh"
 #include "internal.h"
@@ -88,6 +91,28 @@ int ensure_workspace(size_t bytes, void** out) {
         c.ws_bytes = want;
     }
     *out = c.ws;
+    return OPE_OK;
+}
+
+int blocks_per_sm(const void* kernel, int threads, size_t smem, int* per_sm) {
+    static std::mutex mu;
+    static std::map<std::tuple<const void*, int, int, size_t>, int> cache;
+    const auto key = std::make_tuple(kernel, tctx().device, threads, smem);
+    {
+        std::lock_guard<std::mutex> g(mu);
+        const auto it = cache.find(key);
+        if (it != cache.end()) {
+            *per_sm = it->second;
+            return OPE_OK;
+        }
+    }
+    int b = 0;
+    OPE_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    OPE_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, threads, smem));
+    if (b < 1) b = 1;
+    std::lock_guard<std::mutex> g(mu);
+    cache[key] = b;
+    *per_sm = b;
     return OPE_OK;
 }
 

@@ -37,6 +37,10 @@ int check_cuda(cudaError_t e, const char* what);
 int ensure_device();                               // OPE_OK or OPE_ERR_NO_DEVICE
 int ensure_workspace(size_t bytes, void** out);    // grows the per-thread workspace
 int ensure_pinned(size_t bytes, void** out);       // grows the pinned staging buffer
+// Resident blocks per SM of `kernel` (threads per block, dynamic shared
+// memory) on the current device, with its dynamic-shared-memory attribute
+// set; queried once per kernel and device, then cached.
+int blocks_per_sm(const void* kernel, int threads, size_t smem, int* per_sm);
 
 // Profiler ranges (NVTX, header-only: free when no tool is attached), one
 // per C-ABI call and per server micro-batch.

@@ -169,9 +169,7 @@ __global__ void __launch_bounds__(OPE_KERNEL_WARPS * 32, OPE_KERNEL_MINB) k_pric
 template <class K>
 int persistent_grid(K kernel, int threads, size_t smem, int* grid) {
     int per_sm = 0;
-    OPE_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    OPE_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem));
-    if (per_sm < 1) per_sm = 1;
+    OPE_TRY(blocks_per_sm(reinterpret_cast<const void*>(kernel), threads, smem, &per_sm));
     *grid = std::max(1, (int)(per_sm * tctx().sm_count * tctx().grid_fraction));
     return OPE_OK;
 }
@@ -200,8 +198,14 @@ int launch_price_persistent(int model, const ope_contract* con, size_t n, const 
                             const PriceScratch& s, cudaStream_t st, int32_t* nbis_out, const int32_t* surf_mask,
                             const PanelSink* sink) {
     if (n == 0) return OPE_OK;
-    OPE_CHECK(cudaMemsetAsync(s.done, 0, n * sizeof(unsigned int), st));
-    OPE_CHECK(cudaMemsetAsync(s.head, 0, sizeof(unsigned long long), st));
+    // completion counters and queue head start at zero (one memset when adjacent)
+    const size_t done_bytes = align_up(n * sizeof(unsigned int), 256);
+    if (reinterpret_cast<char*>(s.head) == reinterpret_cast<char*>(s.done) + done_bytes) {
+        OPE_CHECK(cudaMemsetAsync(s.done, 0, done_bytes + sizeof(unsigned long long), st));
+    } else {
+        OPE_CHECK(cudaMemsetAsync(s.done, 0, n * sizeof(unsigned int), st));
+        OPE_CHECK(cudaMemsetAsync(s.head, 0, sizeof(unsigned long long), st));
+    }
     const bool bates = model == OPE_MODEL_BATES;
     if (sink) {
         OPE_TRY((bates ? launch_impl<true, true> : launch_impl<false, true>)(
