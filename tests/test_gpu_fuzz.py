@@ -138,3 +138,38 @@ def test_wide_range_implied_vol(ope, oracle):
     err = np.abs(got[both] - ref[both]) / (2.5e-10 / np.maximum(vega, 1e-300) + 1e-12)
     print(f"implied vol: {both.sum()} of {n} compared, worst error / bar = {err.max():.3g}")
     assert err.max() <= 1.0
+
+
+def test_wide_range_calibration(ope, oracle):
+    """calibration.rs:433-569 on 12 random Heston surfaces (true parameters over
+    wide, Feller-respecting ranges, IV noise of 0.2 vol points, perturbed
+    starts): the device LM against the oracle running the same LM with the
+    same exact Jacobian (jac_mode=1).  Where both converge they must reach the
+    same fit; both must stop for the same reason on most surfaces."""
+    rng = np.random.default_rng(901)
+    agree = 0
+    for k in range(12):
+        while True:
+            tp = np.array([rng.uniform(0.01, 0.3), rng.uniform(0.3, 8.0), rng.uniform(0.01, 0.3),
+                           rng.uniform(0.1, 1.5), rng.uniform(-0.95, 0.5)])
+            if 2 * tp[1] * tp[2] > tp[3] ** 2:
+                break
+        rows = []
+        for t in (0.1, 0.5, 1.0, 2.0):
+            for m in (-0.4, -0.2, -0.1, 0.0, 0.1, 0.2, 0.3):
+                rows.append((S, S * np.exp(m), t, 0.02, 0.01, 0.2, 0 if m >= 0 else 1, 0))
+        con = np.array(rows, dtype=W.CONTRACT_DTYPE)
+        px = oracle.batch_price(con, tp, False, 1e-10)
+        iv, ok = oracle.batch_implied_vol(con, px)
+        con, iv = con[ok.astype(bool)], iv[ok.astype(bool)] + rng.normal(0.0, 0.002, ok.sum())
+        p0 = tp * rng.uniform(0.8, 1.2, 5)
+        p0[3] = min(p0[3], 0.95 * np.sqrt(2 * p0[1] * p0[2]))
+        g = ope.calibrate_heston(con, iv, p0)
+        o = oracle.calibrate_ex(5, con, iv, p0, jac_mode=1)
+        if g["converged"] and o["converged"]:
+            assert abs(g["rmse"] - o["rmse"]) < 1e-9, (k, g["rmse"], o["rmse"])
+            assert np.allclose(g["params"][:5], o["params"][:5], rtol=1e-5, atol=1e-8), (k, g["params"][:5],
+                                                                                        o["params"][:5])
+        agree += int(g["converged"] == o["converged"] and g["early_stopped"] == o["early_stopped"])
+    print(f"calibration: {agree} of 12 surfaces stop the same way")
+    assert agree >= 10
