@@ -544,7 +544,8 @@ def run_ours(args) -> None:
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, m, dt, cores, worst = cpu_sample(w, args.cpu_seconds, gpu_prices=ref_prices)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
-                                "sample": f"{m} random contracts of the workload in {dt:.1f} s"}
+                                "sample": f"{m} random contracts of the workload in {dt:.1f} s",
+                                "host_nproc": os.cpu_count()}
         line["parity"] = {"max_abs_err_over_spot": worst, "bar": 1e-9, "contracts_checked": m,
                           "against": "CPU oracle (the reference restated), same tolerance, same contracts"}
     if rank == 0 and world == 1 and not args.no_gradient:
