@@ -545,7 +545,7 @@ def run_ours(args) -> None:
         rate, m, dt, cores, worst = cpu_sample(w, args.cpu_seconds, gpu_prices=ref_prices)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
                                 "sample": f"{m} random contracts of the workload in {dt:.1f} s",
-                                "host_nproc": os.cpu_count()}
+                                "host_cpus_available": len(os.sched_getaffinity(0))}
         line["parity"] = {"max_abs_err_over_spot": worst, "bar": 1e-9, "contracts_checked": m,
                           "against": "CPU oracle (the reference restated), same tolerance, same contracts"}
     if rank == 0 and world == 1 and not args.no_gradient:
