@@ -354,6 +354,69 @@ def bench_gradient(args, w, dev, flush, stream, price_kernel_ms) -> dict:
     return out
 
 
+def bench_greeks(args, w, dev, flush, stream) -> dict:
+    """greeks.rs:19-72 (bump-and-reprice, 14 pricings per contract) and
+    ad.rs:736-865 (AD Greeks: 9 pricings + 3 adjoint evaluations per contract)
+    on 65,536 contracts of the pricing workload under one parameter set
+    (surface 0's), device-resident, L2 flushed, CUDA events."""
+    import ctypes
+
+    import torch
+
+    import ope_b200 as ope
+
+    n = min(65536, w.n)
+    con = w.contracts[:n]
+    par = w.params[0]
+    d_con = torch.from_numpy(con.view(np.uint8).copy()).to(dev)
+    d_par = torch.from_numpy(par.copy()).to(dev)
+    d_out = torch.empty(n * 8, dtype=torch.float64, device=dev)
+    lib = ope._lib.load()
+
+    def run(fn):
+        o = ope._lib.Options(tol=w.tol, flags=ope._lib.FLAG_DEVICE_PTRS, reserved=0, stream=stream.cuda_stream)
+        ope._lib.check(fn(ope.MODEL_BATES, d_con.data_ptr(), n, d_par.data_ptr(), d_out.data_ptr(),
+                          ctypes.byref(o)))
+
+    out = {"workload": f"c3-bates-deepwing first {n} contracts, surface 0's parameters", "n_contracts": n}
+    for name, fn in (("bump", lib.ope_batch_greeks_ex), ("ad", lib.ope_batch_greeks_ad)):
+        for _ in range(max(args.warmup, 3)):
+            flush.zero_()
+            run(fn)
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(args.steps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            run(fn)
+            b.record(stream)
+            torch.cuda.synchronize()
+            ms.append(a.elapsed_time(b))
+        out[name] = {"value": n / (statistics.mean(ms) * 1e-3), "unit": "contracts/s (8 Greeks each)",
+                     "ms": statistics.mean(ms)}
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+
+        rng = np.random.default_rng(5)
+        pick = np.sort(rng.choice(n, 512, replace=False))
+        t0 = time.perf_counter()
+        ref = O.batch_greeks(con[pick], par, True, tol=w.tol)
+        dt = time.perf_counter() - t0
+        bump = ope.batch_bates_greeks(con[pick], par, tol=w.tol)
+        out["bump"]["cpu_baseline"] = {"value": pick.size / dt, "unit": out["bump"]["unit"], "cores": O.max_threads(),
+                                       "kind": "port", "sample": f"{pick.size} contracts, {dt:.1f} s"}
+        out["bump"]["max_abs_price_err_over_spot"] = float(np.max(np.abs(bump["price"] - ref[:, 0])) / 100.0)
+        t0 = time.perf_counter()
+        refad = np.array([O.greeks_ad(c, par, True, w.tol) for c in con[pick[:64]]])
+        dt = time.perf_counter() - t0
+        ad = ope.batch_greeks_ad(ope.MODEL_BATES, con[pick[:64]], par, tol=w.tol)
+        out["ad"]["cpu_baseline"] = {"value": 64 / dt, "unit": out["ad"]["unit"], "cores": 1, "kind": "port",
+                                     "sample": f"64 contracts, one thread, {dt:.1f} s"}
+        out["ad"]["max_abs_vega_rel_err"] = float(np.max(np.abs(ad["vega"] - refad[:, 3]) / np.abs(refad[:, 3])))
+    return out
+
+
 def bench_serving(args) -> dict:
     """Config 5: Poisson arrivals, 80 % Bates surface reprices / 20 % Heston
     calibrations, sizes log-uniform in [20, 2000] contracts, rates swept."""
@@ -550,6 +613,8 @@ def run_ours(args) -> None:
                           "against": "CPU oracle (the reference restated), same tolerance, same contracts"}
     if rank == 0 and world == 1 and not args.no_gradient:
         line["gradient"] = bench_gradient(args, w, dev, flush, stream, kern_avg)
+    if rank == 0 and world == 1 and not args.no_gradient:
+        line["greeks"] = bench_greeks(args, w, dev, flush, stream)
     if rank == 0 and world == 1 and not args.no_calib:
         line["calibration"] = bench_calibration(args)
     if rank == 0 and world == 1 and not args.no_serving:
