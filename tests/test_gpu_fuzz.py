@@ -173,3 +173,29 @@ def test_wide_range_calibration(ope, oracle):
         agree += int(g["converged"] == o["converged"] and g["early_stopped"] == o["early_stopped"])
     print(f"calibration: {agree} of 12 surfaces stop the same way")
     assert agree >= 10
+
+
+@pytest.mark.parametrize("bates", [False, True])
+def test_extreme_inputs_parity(ope, oracle, bates):
+    """Corners: tolerance 1e-12 (the 200-panel cap binds often), expiries down
+    to 1e-4 years, log-moneyness out to +-4, zero rates, near-zero v0 and
+    theta.  Same finiteness and the 1e-9 S bar."""
+    rng = np.random.default_rng(1301 + bates)
+    n = 4000
+    con, p = _draw(rng, n, bates)
+    t = np.exp(rng.uniform(np.log(1e-4), np.log(10.0), n))
+    con["expiry"] = t
+    con["strike"] = S * np.exp(rng.uniform(-4.0, 4.0, n))
+    zero = rng.random(n) < 0.2
+    con["rate"][zero], con["div_yield"][zero] = 0.0, 0.0
+    small = rng.random(n) < 0.2
+    p[small, 0] = rng.uniform(1e-6, 1e-4, small.sum())
+    p[small, 2] = rng.uniform(1e-6, 1e-4, small.sum())
+    off = np.arange(n + 1, dtype=np.int64)
+    got = ope.price_surfaces(ope.MODEL_BATES if bates else ope.MODEL_HESTON, con, off, p, tol=1e-12)
+    ref = oracle.batch_price(con, p, bates, 1e-12, surf_idx=np.arange(n, dtype=np.int32))
+    fin = np.isfinite(ref)
+    assert np.array_equal(np.isfinite(got), fin)
+    err = np.abs(got[fin] - ref[fin])
+    print(f"bates={bates} extreme: {fin.sum()} finite of {n}, worst |gpu - oracle| / S = {err.max() / S:.2e}")
+    assert err.max() <= 1e-9 * S
