@@ -17,9 +17,12 @@
  *    (heston.rs:193-212); the absolute tolerance defaults to the reference's
  *    hard-coded 1e-8 (heston.rs:228) and is settable through ope_options.tol.
  *  - Thread safety: calls may come from any host thread.  Each thread owns
- *    a private device workspace; asynchronous (device-pointer) calls issued
- *    from ONE thread on DIFFERENT streams must not overlap in time, because
- *    they share that thread's workspace.
+ *    a private device workspace.  Calls of one thread are ordered through
+ *    it: a call whose work goes to a different stream than the previous
+ *    call's (a device-pointer call on another stream, or a host-pointer call
+ *    after a device-pointer one) first makes its stream wait, on the device,
+ *    for the previous call's work.  Calls from different threads run
+ *    independently.
  *  - Single GPU: the current CUDA device of the calling thread.
  */
 #ifndef OPE_H

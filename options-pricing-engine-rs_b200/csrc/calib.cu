@@ -764,12 +764,12 @@ int run_calibration(int model, const ope_contract* quotes, const double* iv_mark
                     bool device_ptrs, cudaStream_t ust, const CalibExtra* ex) {
     ThreadCtx& c = tctx();
     const int dim = param_stride(model);
-    void* ws;
-    OPE_TRY(ensure_workspace(calib_workspace_bytes(nq, ns, dim), &ws));
-    void* pin;
-    OPE_TRY(ensure_pinned(calib_pinned_bytes(nq, ns, dim), &pin));
     cudaStream_t st = device_ptrs ? ust : c.stream;
     if (device_ptrs && st == nullptr) st = c.stream;  // capture needs a non-legacy stream
+    void* ws;
+    OPE_TRY(ensure_workspace(calib_workspace_bytes(nq, ns, dim), &ws, st));
+    void* pin;
+    OPE_TRY(ensure_pinned(calib_pinned_bytes(nq, ns, dim), &pin));
     std::vector<int64_t> off_h(ns + 1);
     if (device_ptrs) {
         OPE_CHECK(cudaMemcpyAsync(off_h.data(), surf_offsets, (ns + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
@@ -813,10 +813,10 @@ int run_calib_jacobian(int model, const ope_contract* quotes, const double* iv_m
     ThreadCtx& c = tctx();
     const int dim = param_stride(model);
     const Layout L = layout(nq, ns, dim);
-    void* ws;
-    OPE_TRY(ensure_workspace(L.total, &ws));
-    char* base = static_cast<char*>(ws);
     cudaStream_t st = c.stream;
+    void* ws;
+    OPE_TRY(ensure_workspace(L.total, &ws, st));
+    char* base = static_cast<char*>(ws);
     std::vector<int32_t> sidx(nq);
     for (size_t s = 0; s < ns; ++s)
         for (int64_t i = surf_offsets[s]; i < surf_offsets[s + 1]; ++i) sidx[i] = (int32_t)s;

@@ -508,10 +508,10 @@ int run_global(int model, const ope_contract* quotes, const double* iv_market, c
                  o_price = take(nr * sizeof(double)), o_res = take(nr * sizeof(double)),
                  o_state = take(4 * sizeof(int)), o_bsse = take(ns * sizeof(double)),
                  o_win = take(ns * dim * sizeof(double)), o_scr = take(price_scratch_bytes(nr));
-    void* ws;
-    OPE_TRY(ensure_workspace(o, &ws));
-    char* b = static_cast<char*>(ws);
     cudaStream_t st = c.stream;
+    void* ws;
+    OPE_TRY(ensure_workspace(o, &ws, st));
+    char* b = static_cast<char*>(ws);
     OPE_CHECK(cudaMemcpyAsync(b + o_con, con.data(), nr * sizeof(ope_contract), cudaMemcpyHostToDevice, st));
     OPE_CHECK(cudaMemcpyAsync(b + o_unit, unit.data(), nr * sizeof(int32_t), cudaMemcpyHostToDevice, st));
     OPE_CHECK(cudaMemcpyAsync(b + o_qidx, qidx.data(), nr * sizeof(int32_t), cudaMemcpyHostToDevice, st));

@@ -71,8 +71,19 @@ int ensure_device() {
     return OPE_OK;
 }
 
-int ensure_workspace(size_t bytes, void** out) {
+ApiScope::ApiScope() { ++tctx().api_depth; }
+
+ApiScope::~ApiScope() {
     ThreadCtx& c = tctx();
+    if (--c.api_depth == 0 && c.ws_taken) {
+        c.ws_taken = false;
+        c.ws_recorded = cudaEventRecord(c.ws_event, c.ws_stream) == cudaSuccess;
+    }
+}
+
+int ensure_workspace(size_t bytes, void** out, cudaStream_t st) {
+    ThreadCtx& c = tctx();
+    if (!c.ws_event) OPE_CHECK(cudaEventCreateWithFlags(&c.ws_event, cudaEventDisableTiming));
     if (c.ws_limit && bytes > c.ws_limit)
         return set_error(OPE_ERR_OUT_OF_MEMORY, "call needs " + std::to_string(bytes) +
                                                     " bytes of device workspace, above this thread's limit of " +
@@ -83,6 +94,7 @@ int ensure_workspace(size_t bytes, void** out) {
             OPE_CHECK(cudaFree(c.ws));
             c.ws = nullptr;
             c.ws_bytes = 0;
+            c.ws_recorded = false;  // nothing in flight uses the old one
         }
         size_t want = std::max(bytes, c.ws_bytes + c.ws_bytes / 2);
         want = align_up(want, 1 << 20);
@@ -90,6 +102,9 @@ int ensure_workspace(size_t bytes, void** out) {
         OPE_CHECK(cudaMalloc(&c.ws, want));
         c.ws_bytes = want;
     }
+    if (c.ws_recorded && c.ws_stream != st) OPE_CHECK(cudaStreamWaitEvent(st, c.ws_event, 0));
+    c.ws_stream = st;
+    c.ws_taken = true;
     *out = c.ws;
     return OPE_OK;
 }
@@ -179,14 +194,14 @@ int batch_price(int32_t model, const ope_contract* contracts, size_t n, const vo
     const int stride = param_stride(model);
     if (device_ptrs(opts)) {
         void* ws;
-        OPE_TRY(ensure_workspace(price_scratch_bytes(n), &ws));
+        OPE_TRY(ensure_workspace(price_scratch_bytes(n), &ws, user_stream(opts)));
         return launch_price_persistent(model, contracts, n, nullptr, 1, nullptr, static_cast<const double*>(params),
                                        tol, out, carve_price_scratch(ws, n), user_stream(opts));
     }
     ThreadCtx& c = tctx();
     const size_t b_con = align_up(n * sizeof(ope_contract), 256), b_par = 256, b_out = align_up(n * sizeof(double), 256);
     void* ws;
-    OPE_TRY(ensure_workspace(b_con + b_par + b_out + price_scratch_bytes(n), &ws));
+    OPE_TRY(ensure_workspace(b_con + b_par + b_out + price_scratch_bytes(n), &ws, c.stream));
     char* p = static_cast<char*>(ws);
     ope_contract* d_con = reinterpret_cast<ope_contract*>(p);
     double* d_par = reinterpret_cast<double*>(p + b_con);
@@ -223,14 +238,14 @@ int batch_greeks(int32_t model, const ope_contract* contracts, size_t n, const v
     };
     if (device_ptrs(opts)) {
         void* ws;
-        OPE_TRY(ensure_workspace(g_bytes, &ws));
+        OPE_TRY(ensure_workspace(g_bytes, &ws, user_stream(opts)));
         return launch(contracts, static_cast<const double*>(params), out, ws, user_stream(opts));
     }
     ThreadCtx& c = tctx();
     const size_t b_con = align_up(n * sizeof(ope_contract), 256), b_par = 256,
                  b_out = align_up(n * sizeof(ope_pricing_result), 256);
     void* ws;
-    OPE_TRY(ensure_workspace(b_con + b_par + b_out + g_bytes, &ws));
+    OPE_TRY(ensure_workspace(b_con + b_par + b_out + g_bytes, &ws, c.stream));
     char* p = static_cast<char*>(ws);
     ope_contract* d_con = reinterpret_cast<ope_contract*>(p);
     double* d_par = reinterpret_cast<double*>(p + b_con);
@@ -354,7 +369,7 @@ int ope_batch_implied_vol(const ope_contract* contracts, size_t n, const double*
     const size_t b_con = align_up(n * sizeof(ope_contract), 256), b_d = align_up(n * sizeof(double), 256),
                  b_i = align_up(n * sizeof(int32_t), 256);
     void* ws;
-    OPE_TRY(ensure_workspace(b_con + 2 * b_d + b_i, &ws));
+    OPE_TRY(ensure_workspace(b_con + 2 * b_d + b_i, &ws, c.stream));
     char* p = static_cast<char*>(ws);
     ope_contract* d_con = reinterpret_cast<ope_contract*>(p);
     double* d_px = reinterpret_cast<double*>(p + b_con);
@@ -475,7 +490,7 @@ int ope_price_gradient_surfaces(int32_t model, const ope_contract* contracts, si
     const int dim = param_stride(model);
     if (device_ptrs(opts)) {
         void* ws;
-        OPE_TRY(ensure_workspace(grad_scratch_bytes(n, dim), &ws));
+        OPE_TRY(ensure_workspace(grad_scratch_bytes(n, dim), &ws, user_stream(opts)));
         return launch_price_grad(model, contracts, n, surf_offsets, n_surf, nullptr, static_cast<const double*>(params),
                                  tol, out_prices, out_grad, ws, user_stream(opts));
     }
@@ -488,7 +503,7 @@ int ope_price_gradient_surfaces(int32_t model, const ope_contract* contracts, si
                  b_par = align_up(n_surf * dim * sizeof(double), 256), b_out = align_up(n * sizeof(double), 256),
                  b_g = align_up(n * dim * sizeof(double), 256);
     void* ws;
-    OPE_TRY(ensure_workspace(b_con + b_off + b_par + b_out + b_g + grad_scratch_bytes(n, dim), &ws));
+    OPE_TRY(ensure_workspace(b_con + b_off + b_par + b_out + b_g + grad_scratch_bytes(n, dim), &ws, c.stream));
     char* p = static_cast<char*>(ws);
     ope_contract* d_con = reinterpret_cast<ope_contract*>(p);
     int64_t* d_off = reinterpret_cast<int64_t*>(p + b_con);
@@ -507,12 +522,14 @@ int ope_price_gradient_surfaces(int32_t model, const ope_contract* contracts, si
 }
 
 int ope_selftest_math(uint64_t* max_ulp_rcp, uint64_t* max_ulp_sqrt) {
+    OPE_RANGE("ope.selftest_math");
     if (!max_ulp_rcp || !max_ulp_sqrt) return set_error(OPE_ERR_INVALID_ARG, "NULL argument");
     OPE_TRY(ensure_device());
     return selftest_math(max_ulp_rcp, max_ulp_sqrt);
 }
 
 int ope_measure_fp64_peak(double* flops_per_s, double* elapsed_ms) {
+    OPE_RANGE("ope.measure_fp64_peak");
     if (!flops_per_s || !elapsed_ms) return set_error(OPE_ERR_INVALID_ARG, "NULL argument");
     OPE_TRY(ensure_device());
     return measure_fp64_peak(flops_per_s, elapsed_ms);
@@ -538,7 +555,7 @@ int ope_price_surfaces_stats(int32_t model, const ope_contract* contracts, size_
     const int stride = param_stride(model);
     if (device_ptrs(opts)) {
         void* ws;
-        OPE_TRY(ensure_workspace(price_scratch_bytes(n), &ws));
+        OPE_TRY(ensure_workspace(price_scratch_bytes(n), &ws, user_stream(opts)));
         return launch_price_persistent(model, contracts, n, surf_offsets, n_surf, nullptr,
                                        static_cast<const double*>(params), tol, out_prices, carve_price_scratch(ws, n),
                                        user_stream(opts), out_bisections);
@@ -552,7 +569,7 @@ int ope_price_surfaces_stats(int32_t model, const ope_contract* contracts, size_
                  b_par = align_up(n_surf * stride * sizeof(double), 256), b_out = align_up(n * sizeof(double), 256),
                  b_nb = out_bisections ? align_up(2 * n * sizeof(int32_t), 256) : 0;
     void* ws;
-    OPE_TRY(ensure_workspace(b_con + b_off + b_par + b_out + b_nb + price_scratch_bytes(n), &ws));
+    OPE_TRY(ensure_workspace(b_con + b_off + b_par + b_out + b_nb + price_scratch_bytes(n), &ws, c.stream));
     char* p = static_cast<char*>(ws);
     ope_contract* d_con = reinterpret_cast<ope_contract*>(p);
     int64_t* d_off = reinterpret_cast<int64_t*>(p + b_con);

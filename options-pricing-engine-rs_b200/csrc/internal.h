@@ -29,13 +29,24 @@ struct ThreadCtx {
     uint64_t launches = 0;
     size_t ws_limit = 0;         // cap on the device workspace (0: none), ope_set_workspace_limit
     double grid_fraction = 1.0;  // persistent launches fill at most this share of the block slots
+    // Stream order of the workspace: the stream of its last user, an event
+    // recorded there when that user's C-ABI call returned, and whether the
+    // current call has taken the workspace (the event is recorded on exit).
+    cudaStream_t ws_stream = nullptr;
+    cudaEvent_t ws_event = nullptr;
+    bool ws_recorded = false;
+    bool ws_taken = false;
+    int api_depth = 0;
 };
 
 ThreadCtx& tctx();
 int set_error(int code, const std::string& msg);
 int check_cuda(cudaError_t e, const char* what);
 int ensure_device();                               // OPE_OK or OPE_ERR_NO_DEVICE
-int ensure_workspace(size_t bytes, void** out);    // grows the per-thread workspace
+// The per-thread device workspace, grown to `bytes`, for work enqueued on
+// `st`.  If the previous call of this thread used it on another stream, `st`
+// first waits (on the device) for that call's work.
+int ensure_workspace(size_t bytes, void** out, cudaStream_t st);
 int ensure_pinned(size_t bytes, void** out);       // grows the pinned staging buffer
 // Resident blocks per SM of `kernel` (threads per block, dynamic shared
 // memory) on the current device, with its dynamic-shared-memory attribute
@@ -50,7 +61,17 @@ struct NvtxRange {
     NvtxRange(const NvtxRange&) = delete;
     NvtxRange& operator=(const NvtxRange&) = delete;
 };
-#define OPE_RANGE(name) ::ope::NvtxRange _ope_nvtx_range(name)
+// One per C-ABI call: when the outermost call returns, records the
+// workspace's event on the stream its work was enqueued on.
+struct ApiScope {
+    ApiScope();
+    ~ApiScope();
+    ApiScope(const ApiScope&) = delete;
+    ApiScope& operator=(const ApiScope&) = delete;
+};
+#define OPE_RANGE(name)                           \
+    ::ope::NvtxRange _ope_nvtx_range(name);       \
+    ::ope::ApiScope _ope_api_scope
 
 #define OPE_CHECK(call)                                        \
     do {                                                       \

@@ -49,7 +49,7 @@ __global__ void k_selftest_math(unsigned long long* ulp_rcp, unsigned long long*
 int selftest_math(uint64_t* ulp_rcp, uint64_t* ulp_sqrt) {
     ThreadCtx& c = tctx();
     void* ws;
-    OPE_TRY(ensure_workspace(256, &ws));
+    OPE_TRY(ensure_workspace(256, &ws, c.stream));
     unsigned long long* d = static_cast<unsigned long long*>(ws);
     OPE_CHECK(cudaMemsetAsync(d, 0, 2 * sizeof(unsigned long long), c.stream));
     k_selftest_math<<<4096, 256, 0, c.stream>>>(d, d + 1);
@@ -66,7 +66,7 @@ int selftest_math(uint64_t* ulp_rcp, uint64_t* ulp_sqrt) {
 int measure_fp64_peak(double* flops, double* ms) {
     ThreadCtx& c = tctx();
     void* ws;
-    OPE_TRY(ensure_workspace(256, &ws));
+    OPE_TRY(ensure_workspace(256, &ws, c.stream));
     const int threads = 256, blocks = c.sm_count * 4;
     cudaEvent_t e0, e1;
     OPE_CHECK(cudaEventCreate(&e0));

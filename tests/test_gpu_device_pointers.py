@@ -108,3 +108,34 @@ def test_calibration(ope, env, oracle):
     got = host(d_out, ope.CALIB_RESULT_DTYPE, (3,))
     ref = ope.calibrate_surfaces(ope.MODEL_HESTON, con, iv, off, p0)
     assert got.tobytes() == ref.tobytes()
+
+
+def test_calls_on_different_streams_are_ordered(ope, env):
+    """A device-pointer call on one stream, then at once a host-pointer call
+    (the library's own stream) and a device-pointer call on a second stream,
+    all from this thread: they share the thread's workspace, so each later
+    call must wait on the device for the earlier one's work."""
+    torch, st, lib, opts, dev, host = env
+    big = W.c3(n=65536, per_surface=256, seed=47)
+    small = W.c3(n=4096, per_surface=256, seed=48)
+    want_big = ope.price_surfaces(ope.MODEL_BATES, big.contracts, big.surf_offsets, big.params, tol=big.tol)
+    want_small = ope.price_surfaces(ope.MODEL_BATES, small.contracts, small.surf_offsets, small.params, tol=small.tol)
+    st2 = torch.cuda.Stream()
+    o1 = opts(big.tol)
+    o2 = ope._lib.Options(tol=small.tol, flags=ope._lib.FLAG_DEVICE_PTRS, reserved=0, stream=st2.cuda_stream)
+    b = [dev(big.contracts), dev(big.surf_offsets), dev(big.params)]
+    s = [dev(small.contracts), dev(small.surf_offsets), dev(small.params)]
+    for _ in range(3):
+        d_big = torch.full((big.n,), -1.0, dtype=torch.float64, device="cuda")
+        d_small = torch.full((small.n,), -1.0, dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        _ok(ope, lib.ope_price_surfaces(1, b[0].data_ptr(), big.n, b[1].data_ptr(), big.n_surf, b[2].data_ptr(),
+                                        d_big.data_ptr(), ctypes.byref(o1)))
+        got_host = ope.price_surfaces(ope.MODEL_BATES, small.contracts, small.surf_offsets, small.params,
+                                      tol=small.tol)
+        _ok(ope, lib.ope_price_surfaces(1, s[0].data_ptr(), small.n, s[1].data_ptr(), small.n_surf, s[2].data_ptr(),
+                                        d_small.data_ptr(), ctypes.byref(o2)))
+        torch.cuda.synchronize()
+        assert np.array_equal(got_host, want_small)
+        assert np.array_equal(d_big.cpu().numpy(), want_big)
+        assert np.array_equal(d_small.cpu().numpy(), want_small)
