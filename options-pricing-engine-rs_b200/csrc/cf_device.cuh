@@ -187,9 +187,9 @@ __device__ __forceinline__ CfConsts make_consts(double s, double k, double t, do
 // gk_integrate's g(t) (heston.rs:221-227) with the merged-exponent integrand.
 template <bool BATES>
 __device__ __forceinline__ double node_value(const CfConsts& C, double tn) {
-    const double it = rcp_nr(tn);
     const double omt = 1.0 - tn;
-    const double u = omt * it;  // (1 - t) / t
+    const double itt = rcp_nr(omt * tn);  // 1 / ((1 - t) t)
+    const double u = (omt * omt) * itt;   // (1 - t) / t
     const double u2 = u * u;
     // xi = (xr, xi_) ; z = xi^2 + sigma^2 phi(phi+i)
     const double xr = C.xr, xi_ = -C.rs * u;
@@ -247,7 +247,7 @@ __device__ __forceinline__ double node_value(const CfConsts& C, double tn) {
         zim += fma(je, js, -C.ltc * u);
     }
     // Im(e^Z) / u / t^2 = e^{Re Z} sin(Im Z) / ((1 - t) t)
-    const double v = exp(zre) * sin(zim) * rcp_nr(omt * tn);
+    const double v = exp(zre) * sin(zim) * itt;
     const bool ok = (tn > 0.0) && (u >= 1e-12) && isfinite(v);
     return ok ? v : 0.0;
 }

@@ -6,12 +6,12 @@
 // One warp integrates one integral.  Each step bisects the live panel with
 // the largest error estimate: lanes 0-14 evaluate the 15 Kronrod nodes of the
 // left child and lanes 16-30 those of the right child (30 of 32 lanes busy);
-// half-warp shuffle trees reduce the K15 and G7 sums.  The live-panel list
+// a half-warp reduce-scatter forms the K15 and G7 sums.  The live-panel list
 // (at most 200 entries of {err, K, a, b}) sits in shared memory, one list per
 // warp, and is maintained exactly as the reference maintains its Vec:
 //   * argmax by f64::total_cmp with the LAST maximum winning ties (errors are
 //     non-negative, so their IEEE bit patterns compare as unsigned integers
-//     in total_cmp order, and the comparison uses the integer pipe);
+//     in total_cmp order; the warp maximum is three redux.sync steps);
 //   * swap_remove of the chosen panel, then push(left), push(right);
 //   * total += kl + kr - kw; err += el + er - ew, in that association;
 //   * stop when err <= tol or 200 panels are live.
@@ -75,6 +75,10 @@ struct LaneRule {
     double x, wk, wg;
     bool node;  // lane holds a Kronrod node (lane % 16 < 15)
     int half;   // 0 = left child, 1 = right child
+    // reduce-scatter weights: of the K15 and G7 weights of this lane's node,
+    // the one whose product the lane keeps (G7 if lane bit 3 is set) and the
+    // one whose product it sends to lane ^ 8
+    double wkeep, wsend;
 };
 
 __device__ __forceinline__ LaneRule lane_rule(int lane) {
@@ -85,15 +89,31 @@ __device__ __forceinline__ LaneRule lane_rule(int lane) {
     R.wg = c_gk_wg[j];
     R.node = j < 15;
     R.half = lane >> 4;
+    R.wkeep = (lane & 8) ? R.wg : R.wk;
+    R.wsend = (lane & 8) ? R.wk : R.wg;
     return R;
 }
 
-__device__ __forceinline__ void half_warp_sum2(double& a, double& b) {
-#pragma unroll
-    for (int off = 8; off > 0; off >>= 1) {
-        a += __shfl_xor_sync(0xffffffffu, a, off);
-        b += __shfl_xor_sync(0xffffffffu, b, off);
-    }
+// K15 and G7 sums of both children, in every lane.  A reduce-scatter over
+// each half-warp: at the first exchange (lanes i and i^8) the lanes with bit
+// 3 clear keep a K15 partial sum and those with it set a G7 partial sum (each
+// lane sends the product its partner keeps), and three more xor levels
+// finish each sum with one shuffle per level.  Every lane adds the same two
+// partial sums at each level (commuted in its partner), so all lanes of a
+// quarter hold bit-identical totals, summed in the pairing order (8, 4, 2, 1);
+// lanes 0, 8, 16 and 24 then broadcast the four totals.
+__device__ __forceinline__ void gk_sums(double f, const LaneRule& R, double& Kl, double& Gl, double& Kr,
+                                        double& Gr) {
+    const unsigned FULL = 0xffffffffu;
+    double v = R.wkeep * f;
+    v += __shfl_xor_sync(FULL, R.wsend * f, 8);
+    v += __shfl_xor_sync(FULL, v, 4);
+    v += __shfl_xor_sync(FULL, v, 2);
+    v += __shfl_xor_sync(FULL, v, 1);
+    Kl = __shfl_sync(FULL, v, 0);
+    Gl = __shfl_sync(FULL, v, 8);
+    Kr = __shfl_sync(FULL, v, 16);
+    Gr = __shfl_sync(FULL, v, 24);
 }
 
 // Returns the integral (identical in every lane).  `nbis` receives the
@@ -115,10 +135,8 @@ __device__ __forceinline__ double gk_integrate_warp(const CfConsts& C, double to
     while (true) {
         const double c = 0.5 * (pa + pb), h = 0.5 * (pb - pa);
         const double f = active ? node_value<BATES>(C, __dadd_rn(c, __dmul_rn(h, R.x))) : 0.0;
-        double ks = R.wk * f, gs = R.wg * f;
-        half_warp_sum2(ks, gs);
-        const double Kl = __shfl_sync(FULL, ks, 0), Gl = __shfl_sync(FULL, gs, 0);
-        const double Kr = __shfl_sync(FULL, ks, 16), Gr = __shfl_sync(FULL, gs, 16);
+        double Kl, Gl, Kr, Gr;
+        gk_sums(f, R, Kl, Gl, Kr, Gr);
         if (len == 0) {
             const double k0 = __dmul_rn(Kl, 0.5), e0 = __dmul_rn(fabs(Kl - Gl), 0.5);
             if (lane == 0) {
@@ -171,11 +189,15 @@ __device__ __forceinline__ double gk_integrate_warp(const CfConsts& C, double to
                 if (kk >= best) { best = kk; bi = i; }
             }
         }
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-            const unsigned long long ob = __shfl_xor_sync(FULL, best, off);
-            const int oi = __shfl_xor_sync(FULL, bi, off);
-            if (ob > best || (ob == best && oi > bi)) { best = ob; bi = oi; }
+        // warp maximum of the 64-bit keys (high word, then low word among the
+        // lanes holding the top high word), then the largest index holding it
+        {
+            const unsigned hi = (unsigned)(best >> 32), lo = (unsigned)best;
+            const unsigned mh = __reduce_max_sync(FULL, hi);
+            const unsigned ml = __reduce_max_sync(FULL, hi == mh ? lo : 0u);
+            const unsigned mi = __reduce_max_sync(FULL, (hi == mh && lo == ml) ? (unsigned)(bi + 1) : 0u);
+            best = ((unsigned long long)mh << 32) | ml;
+            bi = (int)mi - 1;
         }
         if (!ope_check(bi >= 0 && bi < len, CHK_PANEL_INDEX)) bi = 0;
         w = bi;
