@@ -108,13 +108,15 @@ __global__ void __launch_bounds__(128, OPE_GRAD_MINB) k_grad_backward(const ope_
             const double wj = __shfl_sync(0xffffffffu, R.wk, j & 15);
             if (idx < items) {
                 const bool normaliser = idx == total;
-                double tn = 0.0, hw = 0.0, u = 0.0;
+                double tn = 0.0, hw = 0.0, u = 0.0, itt = 0.0;
                 if (!normaliser) {
                     const double a = __ldg(P + 2 * pi), b = __ldg(P + 2 * pi + 1);
                     const double cc = 0.5 * (a + b), h = 0.5 * (b - a);
                     tn = __dadd_rn(cc, __dmul_rn(h, xj));
                     hw = h * wj;
-                    u = (1.0 - tn) / tn;
+                    const double omt = 1.0 - tn;
+                    itt = rcp_nr(omt * tn);  // 1 / ((1 - t) t), as the pricing node evaluation
+                    u = (omt * omt) * itt;   // (1 - t) / t
                 }
                 C2 dz[8];
                 const C2 Z = exponent_and_grad<BATES>(C, G, u, dz);
@@ -122,7 +124,7 @@ __global__ void __launch_bounds__(128, OPE_GRAD_MINB) k_grad_backward(const ope_
 #pragma unroll
                     for (int k = 0; k < DIM; ++k) { s_norm[warp][2 * k] = dz[k].re; s_norm[warp][2 * k + 1] = dz[k].im; }
                 } else {
-                    node_accumulate<BATES>(Z, dz, tn, u, hw, acc, sw_re, sw_im);
+                    node_accumulate<BATES>(Z, dz, (tn > 0.0) && (u >= 1e-12), itt, hw, acc, sw_re, sw_im);
                 }
             }
         }

@@ -40,8 +40,10 @@ __device__ __forceinline__ C2 operator-(C2 a, C2 b) { return C2{a.re - b.re, a.i
 __device__ __forceinline__ C2 operator*(C2 a, C2 b) { return C2{a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
 __device__ __forceinline__ C2 operator*(C2 a, double s) { return C2{a.re * s, a.im * s}; }
 __device__ __forceinline__ C2 operator*(double s, C2 a) { return C2{a.re * s, a.im * s}; }
+// 1/a with one refined reciprocal (rcp_nr); a = 0 gives a non-finite result,
+// which drops the node as a division by zero does in the reference.
 __device__ __forceinline__ C2 crcp(C2 a) {
-    const double inv = 1.0 / (a.re * a.re + a.im * a.im);
+    const double inv = rcp_nr(a.re * a.re + a.im * a.im);
     return C2{a.re * inv, -a.im * inv};
 }
 
@@ -49,6 +51,7 @@ __device__ __forceinline__ C2 crcp(C2 a) {
 struct GradParams {
     double v0, kappa, theta, sigma, rho;
     double sigma_j;
+    double is2;  // 1 / sigma^2
 };
 
 __device__ __forceinline__ GradParams make_grad_params(const double* p, bool bates) {
@@ -59,6 +62,7 @@ __device__ __forceinline__ GradParams make_grad_params(const double* p, bool bat
     G.sigma = p[3];
     G.rho = p[4];
     G.sigma_j = bates ? p[7] : 0.0;
+    G.is2 = 1.0 / (p[3] * p[3]);
     return G;
 }
 
@@ -70,8 +74,8 @@ __device__ __forceinline__ C2 exponent_and_grad(const CfConsts& C, const GradPar
     const C2 xi = c2(C.kappa + C.rs * C.phi_im, -C.rs * u);
     const C2 wphi = c2(u * u, C.sgn * u);  // phi(phi+i)
     const C2 z = xi * xi + wphi * C.sig2;
-    const Cx dd = fast_csqrt(z.re, z.im);
-    const C2 d = c2(dd.re, dd.im);
+    C2 d;
+    csqrt_node(z.re, z.im, d.re, d.im);
     const C2 m = xi - d, p = xi + d;
     const C2 ip = crcp(p);
     const C2 g = m * ip;
@@ -109,7 +113,7 @@ __device__ __forceinline__ C2 exponent_and_grad(const CfConsts& C, const GradPar
     const C2 Z_z = (C_d + D_d) * crcp(d * 2.0);
     const C2 Y = Z_xi + xi * Z_z * 2.0;
     const C2 s = c2(C.phi_im, -u);
-    const double is2 = 1.0 / C.sig2;
+    const double is2 = P.is2;
     out[0] = Dh * is2;                                                     // v0
     out[1] = Y + Ch * (P.theta * is2);                                     // kappa
     out[2] = Ch * (P.kappa * is2);                                         // theta
@@ -136,21 +140,22 @@ __device__ __forceinline__ C2 exponent_and_grad(const CfConsts& C, const GradPar
 }
 
 // One node of the derivative integral from its exponent Z and dZ/dp (from
-// exponent_and_grad at u = (1 - tn)/tn): adds hw * dg/dp into acc[0..dim)
-// and hw * W/(u t^2) into sw (for the P1 normaliser term).  A node whose
-// value or derivative is not finite contributes zero, as in
-// gk_integrate_dual (ad.rs:679-682).
+// exponent_and_grad at u = (1 - tn)/tn, with itt = 1/((1 - tn) tn) =
+// 1/(u tn^2)): adds hw * dg/dp into acc[0..dim) and hw * W/(u t^2) into sw
+// (for the P1 normaliser term).  A node outside the substitution's domain
+// (`inside` false: t <= 0 or u < 1e-12, heston.rs:222-225) or whose value or
+// derivative is not finite contributes zero, as in gk_integrate_dual
+// (ad.rs:679-682).
 template <bool BATES>
-__device__ __forceinline__ void node_accumulate(const C2& Z, const C2* dz, double tn, double u, double hw,
+__device__ __forceinline__ void node_accumulate(const C2& Z, const C2* dz, bool inside, double itt, double hw,
                                                 double* acc, double& sw_re, double& sw_im) {
     constexpr int DIM = BATES ? 8 : 5;
     double sn, cs;
     sincos(Z.im, &sn, &cs);
     const double ez = exp(Z.re);
-    const double scale = 1.0 / (u * (tn * tn));
-    const C2 Wf = c2(ez * cs * scale, ez * sn * scale);
+    const C2 Wf = c2(ez * cs * itt, ez * sn * itt);
     const double v = Wf.im;
-    bool ok = (tn > 0.0) && (u >= 1e-12) && isfinite(v);
+    bool ok = inside && isfinite(v);
     double gk[8];
 #pragma unroll
     for (int k = 0; k < DIM; ++k) {

@@ -89,6 +89,20 @@ __device__ __forceinline__ Cx fast_csqrt(double a, double b) {
     return (a >= 0.0) ? Cx{w, q} : Cx{fabs(q), copysign(w, b)};
 }
 
+// d = fast_csqrt(z) of the node evaluations (heston.rs:155-175), branch-free
+// and without hypot or a division: w = sqrt((|zr| + |z|)/2) through a
+// refined reciprocal square root, the other component zi / (2 w).  z = 0
+// gives d = 0 as the reference's b == 0 branch does.
+__device__ __forceinline__ void csqrt_node(double zr, double zi, double& dre, double& dim) {
+    const double r = sqrt(fma(zr, zr, zi * zi));
+    const double s2 = 0.5 * (r + fabs(zr));
+    const double iw = rsqrt_nr(s2);
+    const double w = (s2 > 0.0) ? s2 * iw : 0.0;
+    const double q = (s2 > 0.0) ? (0.5 * zi) * iw : zi;
+    dre = (zr >= 0.0) ? w : fabs(q);
+    dim = (zr >= 0.0) ? q : copysign(w, zi);
+}
+
 // Per-integral constants (everything that does not depend on the node),
 // folded so that the node evaluation does as little as possible:
 //   xi   = (xr, -rs u)                       xi = kappa - i rho sigma phi, phi = u + i phi_im
@@ -195,14 +209,8 @@ __device__ __forceinline__ double node_value(const CfConsts& C, double tn) {
     const double xr = C.xr, xi_ = -C.rs * u;
     const double zr = fma(xr, xr, fma(-xi_, xi_, C.sig2 * u2));
     const double zi = fma(2.0 * xr, xi_, C.sig2s * u);
-    // d = fast_csqrt(z) (heston.rs:155-175): w = sqrt((|zr| + |z|)/2), other = zi / (2 w)
-    const double r = sqrt(fma(zr, zr, zi * zi));
-    const double s2 = 0.5 * (r + fabs(zr));
-    const double iw = rsqrt_nr(s2);
-    const double w = (s2 > 0.0) ? s2 * iw : 0.0;
-    const double q = (s2 > 0.0) ? (0.5 * zi) * iw : zi;
-    const double dre = (zr >= 0.0) ? w : fabs(q);
-    const double dim = (zr >= 0.0) ? q : copysign(w, zi);
+    double dre, dim;
+    csqrt_node(zr, zi, dre, dim);
     const double amr = xr - dre, ami = xi_ - dim;  // xi - d
     const double apr = xr + dre, api = xi_ + dim;  // xi + d
     // g = (xi - d) / (xi + d)
