@@ -355,6 +355,12 @@ int ope_price_surfaces_noalloc(int32_t model, const ope_contract* d_contracts, s
  * sqrt over 2^20 inputs spanning 1e-300 .. 1e300. */
 int ope_selftest_math(uint64_t* max_ulp_rcp, uint64_t* max_ulp_sqrt);
 
+/* No reference twin (numerics self-check): the worst difference, in ulps, of
+ * the node evaluation's own branch-free atan2 (used for arg A of the Albrecher
+ * CF, heston.rs:120) from CUDA's atan2 over 2^24 argument pairs with
+ * magnitudes 2^-60 .. 2^60 and ratios 2^-45 .. 2^45. */
+int ope_selftest_atan2(uint64_t* max_ulp);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

@@ -89,7 +89,7 @@ __device__ __forceinline__ C2 exponent_and_grad(const CfConsts& C, const GradPar
     const C2 iM = crcp(M);
     const C2 iN = crcp(N);
     const C2 A = N * iM;
-    const C2 lnA = c2(0.5 * log(A.re * A.re + A.im * A.im), atan2(A.im, A.re));
+    const C2 lnA = c2(0.5 * log(A.re * A.re + A.im * A.im), atan2_node(A.im, A.re));
     const C2 om = c2(1.0 - e.re, -e.im);  // 1 - e
     const C2 iQ = c2(-iN.re, -iN.im);     // 1/(1 - g e)
     const C2 Ch = m * T - lnA * 2.0;

@@ -44,7 +44,42 @@ __global__ void k_selftest_math(unsigned long long* ulp_rcp, unsigned long long*
     atomicMax(ulp_sqrt, (unsigned long long)ds);
 }
 
+// atan2_node against CUDA's atan2 over 2^24 argument pairs: random signs,
+// magnitudes from 2^-60 to 2^60 and ratios |y/x| from 2^-45 to 2^45.
+// Errors in units of the last place of CUDA's result.
+__global__ void k_selftest_atan2(unsigned long long* ulp) {
+    const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long h = 0x9E3779B97F4A7C15ull * (i + 1);
+    h ^= h >> 31;
+    h *= 0xBF58476D1CE4E5B9ull;
+    h ^= h >> 29;
+    unsigned long long g = h * 0x94D049BB133111EBull;
+    g ^= g >> 32;
+    const double m1 = 1.0 + (double)(h >> 12) * 0x1.0p-52, m2 = 1.0 + (double)(g >> 12) * 0x1.0p-52;
+    const int e1 = (int)((h >> 3) % 121) - 60, e2 = (int)((g >> 5) % 91) - 45;
+    const double y = ((h & 1) ? -1.0 : 1.0) * ldexp(m1, e1);
+    const double x = ((h & 2) ? -1.0 : 1.0) * ldexp(m2, e1 + e2);
+    const long long d = llabs(__double_as_longlong(atan2_node(y, x)) - __double_as_longlong(atan2(y, x)));
+    atomicMax(ulp, (unsigned long long)d);
+}
+
 }  // namespace
+
+int selftest_atan2(uint64_t* ulp) {
+    ThreadCtx& c = tctx();
+    void* ws;
+    OPE_TRY(ensure_workspace(256, &ws, c.stream));
+    unsigned long long* d = static_cast<unsigned long long*>(ws);
+    OPE_CHECK(cudaMemsetAsync(d, 0, sizeof(unsigned long long), c.stream));
+    k_selftest_atan2<<<1 << 16, 256, 0, c.stream>>>(d);
+    OPE_CHECK(cudaGetLastError());
+    c.launches += 1;
+    unsigned long long h = 0;
+    OPE_CHECK(cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, c.stream));
+    OPE_CHECK(cudaStreamSynchronize(c.stream));
+    *ulp = h;
+    return OPE_OK;
+}
 
 int selftest_math(uint64_t* ulp_rcp, uint64_t* ulp_sqrt) {
     ThreadCtx& c = tctx();

@@ -287,6 +287,16 @@ def test_newton_reciprocal_and_sqrt_within_two_ulp(ope):
     assert a.value <= 2 and b.value <= 2, (a.value, b.value)
 
 
+def test_own_atan2_within_four_ulp_of_cuda(ope):
+    import ctypes
+
+    from ope_b200 import _lib
+
+    u = ctypes.c_uint64()
+    _lib.check(_lib.load().ope_selftest_atan2(ctypes.byref(u)))
+    assert u.value <= 4, u.value
+
+
 def test_pinned_host_buffers_zero_copy_equal_copy_path(ope):
     """Contracts and prices in pinned host memory are read and written in place
     by the kernel (zero-copy); the prices equal the pageable (copy) path's."""
