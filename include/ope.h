@@ -361,6 +361,12 @@ int ope_selftest_math(uint64_t* max_ulp_rcp, uint64_t* max_ulp_sqrt);
  * magnitudes 2^-60 .. 2^60 and ratios 2^-45 .. 2^45. */
 int ope_selftest_atan2(uint64_t* max_ulp);
 
+/* No reference twin (numerics self-check): the worst difference, in ulps, of
+ * the node evaluation's own log (used for log|A| of the Albrecher CF,
+ * heston.rs:120) from CUDA's log over 2^24 arguments from 2^-1000 to 2^1000
+ * and around 1. */
+int ope_selftest_log(uint64_t* max_ulp);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

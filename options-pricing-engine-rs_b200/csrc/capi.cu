@@ -535,6 +535,13 @@ int ope_selftest_atan2(uint64_t* max_ulp) {
     return selftest_atan2(max_ulp);
 }
 
+int ope_selftest_log(uint64_t* max_ulp) {
+    OPE_RANGE("ope.selftest_log");
+    if (!max_ulp) return set_error(OPE_ERR_INVALID_ARG, "NULL argument");
+    OPE_TRY(ensure_device());
+    return selftest_log(max_ulp);
+}
+
 int ope_measure_fp64_peak(double* flops_per_s, double* elapsed_ms) {
     OPE_RANGE("ope.measure_fp64_peak");
     if (!flops_per_s || !elapsed_ms) return set_error(OPE_ERR_INVALID_ARG, "NULL argument");

@@ -67,7 +67,7 @@ __device__ __forceinline__ double rsqrt_nr(double x) {
 // to atan(q), q = min(|x|,|y|)/max(|x|,|y|) in [0, 1]; above tan(pi/8),
 // atan(q) = pi/4 + atan((q - 1)/(q + 1)); on |t| <= tan(pi/8),
 // atan(t) = t + t s P(s), s = t^2, with the degree-10 Chebyshev interpolant P
-// of atan_coeffs.py (5e-18 relative).  The two quotients use rcp_nr.  At most
+// of node_math_coeffs.py (5e-18 relative).  The two quotients use rcp_nr.  At most
 // 4 ulp from CUDA's atan2 over finite arguments whose larger magnitude is at
 // least 2^-1022 (ope_selftest_atan2); outside that (a NaN or infinite
 // argument, or both below 2^-1022) it returns NaN.  In the node evaluation
@@ -96,6 +96,37 @@ __device__ __forceinline__ double atan2_node(double y, double x) {
     r = swap ? 1.5707963267948966 - r : r;            // first quadrant
     r = (x < 0.0) ? 3.1415926535897931 - r : r;       // upper half plane
     return copysign(r, y);
+}
+
+// log|A|^2 of the node evaluation's Log A: log(v), written for this use
+// (2.4 % off the Bates batch against CUDA's log).  Method (the atanh form of
+// the logarithm of Cody and Waite's manual): v = 2^k m with m in
+// [sqrt(1/2), sqrt 2), read off the IEEE exponent and mantissa bits;
+// log v = k ln 2 + 2 atanh(s), s = (m - 1)/(m + 1) (m - 1 is exact, the
+// quotient uses rcp_nr), 2 atanh(s) = 2 s + s w R(w), w = s^2, with the
+// degree-6 Chebyshev interpolant R of node_math_coeffs.py (4.5e-18 relative),
+// and k ln 2 added through two FMAs with ln 2 split into a double and its
+// remainder.  At most 2 ulp from CUDA's log (ope_selftest_log).  Arguments
+// outside the normal range (0, subnormal, infinite, NaN) take CUDA's log.
+__device__ __forceinline__ double log_node(double v) {
+    const int hi = __double2hiint(v), lo = __double2loint(v);
+    const int k = (hi - 0x3FE6A09E) >> 20;  // 0x3FE6A09E: high word of sqrt(1/2)
+    const double m = __hiloint2double(hi - k * 0x100000, lo);
+    const double f = m - 1.0;
+    const double s = f * rcp_nr(2.0 + f);
+    const double w = s * s;
+    double r = 0.14616449685043406;
+    r = fma(r, w, 0.15331721600556042);
+    r = fma(r, w, 0.18182889125261723);
+    r = fma(r, w, 0.2222221113479508);
+    r = fma(r, w, 0.28571428625975487);
+    r = fma(r, w, 0.39999999999899505);
+    r = fma(r, w, 0.666666666666667);
+    const double lm = fma(s * w, r, 2.0 * s);  // log m
+    const double kd = (double)k;
+    double out = fma(kd, 0.6931471805599453, fma(kd, 2.3190468138462996e-17, lm));
+    if (!(v >= 0x1p-1022 && v <= 0x1.fffffffffffffp+1023)) out = log(v);
+    return out;
 }
 
 __device__ __forceinline__ Cx cadd(Cx a, Cx b) { return Cx{a.re + b.re, a.im + b.im}; }
@@ -270,7 +301,7 @@ __device__ __forceinline__ double node_value(const CfConsts& C, double tn) {
     const double ar = fma(nr, dr, ni * di) * ia;
     const double ai = fma(ni, dr, -nr * di) * ia;
     // Log A
-    const double lr = 0.5 * log(fma(ar, ar, ai * ai));
+    const double lr = 0.5 * log_node(fma(ar, ar, ai * ai));
     const double li = atan2_node(ai, ar);
     // Dh = (xi - d)(1 - e) / (1 - g e)
     const double omr = 1.0 - er, omi = -ei;

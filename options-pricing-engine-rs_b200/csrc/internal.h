@@ -178,6 +178,7 @@ int launch_batch_iv(const ope_contract* con, const double* price, size_t n, doub
 int measure_fp64_peak(double* flops, double* ms);
 int selftest_math(uint64_t* ulp_rcp, uint64_t* ulp_sqrt);
 int selftest_atan2(uint64_t* ulp);
+int selftest_log(uint64_t* ulp);
 // Bump-and-reprice Greeks (greeks.rs:19-72) for n contracts under one
 // parameter set; `ws` must hold greeks_workspace_bytes(n) bytes.
 size_t greeks_workspace_bytes(size_t n);

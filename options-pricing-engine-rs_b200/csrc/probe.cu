@@ -63,7 +63,39 @@ __global__ void k_selftest_atan2(unsigned long long* ulp) {
     atomicMax(ulp, (unsigned long long)d);
 }
 
+// log_node against CUDA's log over 2^24 arguments: half with exponents from
+// 2^-1000 to 2^1000, half in [0.5, 4) around 1.  Errors in units of the last
+// place of CUDA's result.
+__global__ void k_selftest_log(unsigned long long* ulp) {
+    const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long h = 0x9E3779B97F4A7C15ull * (i + 1);
+    h ^= h >> 31;
+    h *= 0xBF58476D1CE4E5B9ull;
+    h ^= h >> 29;
+    const double m = 1.0 + (double)(h >> 12) * 0x1.0p-52;
+    const int e = (i & 1) ? (int)((h >> 3) % 2001) - 1000 : (int)((h >> 3) % 3) - 1;
+    const double v = ldexp(m, e);
+    const long long d = llabs(__double_as_longlong(log_node(v)) - __double_as_longlong(log(v)));
+    atomicMax(ulp, (unsigned long long)d);
+}
+
 }  // namespace
+
+int selftest_log(uint64_t* ulp) {
+    ThreadCtx& c = tctx();
+    void* ws;
+    OPE_TRY(ensure_workspace(256, &ws, c.stream));
+    unsigned long long* d = static_cast<unsigned long long*>(ws);
+    OPE_CHECK(cudaMemsetAsync(d, 0, sizeof(unsigned long long), c.stream));
+    k_selftest_log<<<1 << 16, 256, 0, c.stream>>>(d);
+    OPE_CHECK(cudaGetLastError());
+    c.launches += 1;
+    unsigned long long h = 0;
+    OPE_CHECK(cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, c.stream));
+    OPE_CHECK(cudaStreamSynchronize(c.stream));
+    *ulp = h;
+    return OPE_OK;
+}
 
 int selftest_atan2(uint64_t* ulp) {
     ThreadCtx& c = tctx();

@@ -297,6 +297,16 @@ def test_own_atan2_within_four_ulp_of_cuda(ope):
     assert u.value <= 4, u.value
 
 
+def test_own_log_within_two_ulp_of_cuda(ope):
+    import ctypes
+
+    from ope_b200 import _lib
+
+    u = ctypes.c_uint64()
+    _lib.check(_lib.load().ope_selftest_log(ctypes.byref(u)))
+    assert u.value <= 2, u.value
+
+
 def test_pinned_host_buffers_zero_copy_equal_copy_path(ope):
     """Contracts and prices in pinned host memory are read and written in place
     by the kernel (zero-copy); the prices equal the pageable (copy) path's."""
