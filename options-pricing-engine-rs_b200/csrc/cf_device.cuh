@@ -159,11 +159,13 @@ __device__ __forceinline__ Cx fast_csqrt(double a, double b) {
 }
 
 // d = fast_csqrt(z) of the node evaluations (heston.rs:155-175), branch-free
-// and without hypot or a division: w = sqrt((|zr| + |z|)/2) through a
-// refined reciprocal square root, the other component zi / (2 w).  z = 0
-// gives d = 0 as the reference's b == 0 branch does.
+// and without hypot, a division or an IEEE square root: |z| and
+// w = sqrt((|zr| + |z|)/2) through refined reciprocal square roots, the other
+// component zi / (2 w).  z = 0 gives d = 0 as the reference's b == 0 branch
+// does.
 __device__ __forceinline__ void csqrt_node(double zr, double zi, double& dre, double& dim) {
-    const double r = sqrt(fma(zr, zr, zi * zi));
+    const double zz = fma(zr, zr, zi * zi);
+    const double r = (zz > 0.0) ? zz * rsqrt_nr(zz) : zz;  // |z| (zz = 0 stays 0)
     const double s2 = 0.5 * (r + fabs(zr));
     const double iw = rsqrt_nr(s2);
     const double w = (s2 > 0.0) ? s2 * iw : 0.0;
@@ -297,18 +299,30 @@ __device__ __forceinline__ double node_value(const CfConsts& C, double tn) {
     // A = (g e - 1) / (g - 1)
     const double nr = ger - 1.0, ni = gei;
     const double dr = gr - 1.0, di = gi;
-    const double ia = rcp_nr(fma(dr, dr, di * di));
-    const double ar = fma(nr, dr, ni * di) * ia;
-    const double ai = fma(ni, dr, -nr * di) * ia;
-    // Log A
-    const double lr = 0.5 * log_node(fma(ar, ar, ai * ai));
-    const double li = atan2_node(ai, ar);
+    const double mm = fma(dr, dr, di * di);
+    double lr, li, iqc;
+    if (BATES) {
+        // |A|^2 = |N|^2/|M|^2 and 1/|1 - g e|^2 = 1/|N|^2 from one reciprocal;
+        // arg A = arg(N conj(M)) (faster for the Bates instantiation only)
+        const double nn = fma(nr, nr, ni * ni);
+        const double inv = rcp_nr(nn * mm);
+        lr = 0.5 * log_node((nn * nn) * inv);
+        li = atan2_node(fma(ni, dr, -nr * di), fma(nr, dr, ni * di));
+        iqc = mm * inv;
+    } else {
+        const double ia = rcp_nr(mm);
+        const double ar = fma(nr, dr, ni * di) * ia;
+        const double ai = fma(ni, dr, -nr * di) * ia;
+        lr = 0.5 * log_node(fma(ar, ar, ai * ai));
+        li = atan2_node(ai, ar);
+        iqc = 0.0;
+    }
     // Dh = (xi - d)(1 - e) / (1 - g e)
     const double omr = 1.0 - er, omi = -ei;
     const double pr = fma(amr, omr, -ami * omi);
     const double pim = fma(amr, omi, ami * omr);
     const double qr = 1.0 - ger, qi = -gei;
-    const double iq = rcp_nr(fma(qr, qr, qi * qi));
+    const double iq = BATES ? iqc : rcp_nr(fma(qr, qr, qi * qi));
     const double Dr = fma(pr, qr, pim * qi) * iq;
     const double Di = fma(pim, qr, -pr * qi) * iq;
     // Ch = (xi - d) T - 2 Log A
