@@ -18,17 +18,17 @@
 
 // Launch shape of the pricing kernel: warps per block and, per model, the
 // minimum resident blocks per SM handed to __launch_bounds__ (which caps
-// registers per thread at 65536 / (32 * WARPS * MINB)): 72 registers x 7
-// blocks for Bates, 80 x 6 for Heston (the faster of 6/7/8 on each model's
-// full batch; Bates is flat across them, Heston 2.8 % faster at 6).
+// registers per thread at 65536 / (32 * WARPS * MINB)): 64 registers x 8
+// blocks for Bates, 72 x 7 for Heston, each the fastest of 6/7/8 blocks on
+// its model's full batch (within 2 % of one another).
 #ifndef OPE_KERNEL_WARPS
 #define OPE_KERNEL_WARPS 4
 #endif
 #ifndef OPE_KERNEL_MINB_BATES
-#define OPE_KERNEL_MINB_BATES 7
+#define OPE_KERNEL_MINB_BATES 8
 #endif
 #ifndef OPE_KERNEL_MINB_HESTON
-#define OPE_KERNEL_MINB_HESTON 6
+#define OPE_KERNEL_MINB_HESTON 7
 #endif
 
 namespace ope {
