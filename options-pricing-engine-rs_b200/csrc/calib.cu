@@ -491,7 +491,7 @@ thread_local CalibGraph g_lm_graph;
 struct Layout {
     size_t total;
     size_t q, iv, w, off, sidx, st, pcur, ptrial, jmask, tmask, price, price_trial, jslot, pslot, pgrad, res, res_new,
-        jrow, counters, out, prior, regw, group, gbest, sink, ginteg, bhead, scratch;
+        jrow, counters, out, prior, regw, group, gbest, sink, bscr, scratch;
 };
 
 Layout layout(size_t nq, size_t ns, int dim) {
@@ -523,8 +523,7 @@ Layout layout(size_t nq, size_t ns, int dim) {
     L.group = take(ns * sizeof(int32_t));
     L.gbest = take(ns * sizeof(unsigned long long));
     L.sink = take(panel_sink_bytes(nq, 2));
-    L.ginteg = take(2 * nq * dim * sizeof(double));
-    L.bhead = take(sizeof(unsigned long long));
+    L.bscr = take(grad_backward_bytes(nq, dim));
     L.scratch = take(price_scratch_bytes(nq));
     L.total = o;
     return L;
@@ -570,9 +569,8 @@ PanelSink pricing_sink(const LMDev& D, char* base, const Layout& L) {
 // adjoint's backward pass over the panel lists of the current slot.
 int launch_jac(int model, const LMDev& D, char* base, const Layout& L, cudaStream_t st) {
     const PanelSink src = carve_panel_sink(base + L.sink, D.nq, 2, D.jslot);
-    OPE_TRY(launch_grad_backward(model, D.q, D.nq, D.off, D.ns, nullptr, D.pcur, src,
-                                 reinterpret_cast<double*>(base + L.ginteg),
-                                 reinterpret_cast<unsigned long long*>(base + L.bhead), D.pgrad, st, D.jmask));
+    OPE_TRY(launch_grad_backward(model, D.q, D.nq, D.off, D.ns, nullptr, D.pcur, src, base + L.bscr, D.pgrad, st,
+                                 D.jmask));
     k_lm_jrows<<<(D.nq + 127) / 128, 128, 0, st>>>(D);
     OPE_CHECK(cudaGetLastError());
     tctx().launches += 1;

@@ -124,11 +124,11 @@ int launch_price_persistent(int model, const ope_contract* con, size_t n, const 
                             const int32_t* surf_mask = nullptr, const PanelSink* sink = nullptr);
 // The adjoint's backward pass and combine (adjoint.cu) over panel lists a
 // pricing launch stored in `src`: out_grad (n x dim) = d price / d params.
-// ginteg: 2n x dim doubles; head: one zeroed-on-launch queue counter.
+// bscratch: grad_backward_bytes(n, dim) bytes (chunk list, partial sums).
+size_t grad_backward_bytes(size_t n, int dim);
 int launch_grad_backward(int model, const ope_contract* con, size_t n, const int64_t* surf_offsets, size_t n_surf,
-                         const int32_t* param_idx, const double* params, const PanelSink& src, double* ginteg,
-                         unsigned long long* head, double* out_grad, cudaStream_t st,
-                         const int32_t* surf_mask = nullptr);
+                         const int32_t* param_idx, const double* params, const PanelSink& src, void* bscratch,
+                         double* out_grad, cudaStream_t st, const int32_t* surf_mask = nullptr);
 // Price + reverse-mode parameter gradient (adjoint.cu); `scratch` must hold
 // grad_scratch_bytes(n, dim) bytes; out_grad is n x dim (dim 5 or 8).
 size_t grad_scratch_bytes(size_t n, int dim);
