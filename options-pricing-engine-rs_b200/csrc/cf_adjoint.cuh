@@ -51,7 +51,8 @@ __device__ __forceinline__ C2 crcp(C2 a) {
 struct GradParams {
     double v0, kappa, theta, sigma, rho;
     double sigma_j;
-    double is2;  // 1 / sigma^2
+    double is2;     // 1 / sigma^2
+    double sk, sv;  // 2 kts / sigma and 2 v0s / sigma (kts, v0s as in make_consts)
 };
 
 __device__ __forceinline__ GradParams make_grad_params(const double* p, bool bates) {
@@ -63,6 +64,8 @@ __device__ __forceinline__ GradParams make_grad_params(const double* p, bool bat
     G.rho = p[4];
     G.sigma_j = bates ? p[7] : 0.0;
     G.is2 = 1.0 / (p[3] * p[3]);
+    G.sk = 2.0 * ((p[1] * p[2]) / (p[3] * p[3])) / p[3];
+    G.sv = 2.0 * (p[0] / (p[3] * p[3])) / p[3];
     return G;
 }
 
@@ -117,8 +120,7 @@ __device__ __forceinline__ C2 exponent_and_grad(const CfConsts& C, const GradPar
     out[0] = Dh * is2;                                                     // v0
     out[1] = Y + Ch * (P.theta * is2);                                     // kappa
     out[2] = Ch * (P.kappa * is2);                                         // theta
-    out[3] = Y * s * P.rho + Z_z * wphi * (2.0 * P.sigma) - Ch * (2.0 * C.kts / P.sigma) -
-             Dh * (2.0 * C.v0s / P.sigma);                                 // sigma
+    out[3] = Y * s * P.rho + Z_z * wphi * (2.0 * P.sigma) - Ch * P.sk - Dh * P.sv;  // sigma
     out[4] = Y * s * P.sigma;                                              // rho
     if (BATES) {
         const C2 iphi = c2(-C.phi_im, u);
