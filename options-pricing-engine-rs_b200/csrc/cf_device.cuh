@@ -257,12 +257,28 @@ __device__ __forceinline__ CfConsts make_consts(double s, double k, double t, do
     C.lnm_re = 0.0;
     C.lnm_im = 0.0;
     if (which == 0) {
-        const Cx phi_mi{0.0, -1.0};
-        Cx m = stable_cf_ref(phi_mi, t, r, v0, kappa, theta, sigma, rho);
-        if (bates) m = cmul(m, jump_cf_ref(phi_mi, t, p[5], p[6], p[7]));
-        Cx lm = clog(m);
-        C.lnm_re = -lm.re;
-        C.lnm_im = -lm.im;
+        // CF(-i) = e^{rT} in exact arithmetic (C = D = 0 there, jump factor 1),
+        // and the reference's operation sequence reproduces that to the last
+        // ulp or so whenever xi(-i) = kappa - rho sigma (C.xr) is a positive
+        // normal number and the other terms are moderate: then Log CF(-i) is
+        // rT.  Everywhere else -- xi(-i) <= 0, where xi + d = 0 makes the
+        // reference's CF(-i) NaN and drops every P1 node, and any extreme or
+        // non-finite parameter -- it is evaluated with the reference's own
+        // sequence.  (The regular case skips two complex exponentials, three
+        // complex divisions and two complex logarithms per P1 integral.)
+        bool regular = C.xr > 1e-100 && C.xr < 1e100 && C.sig2 > 1e-100 && C.kts < 1e4 &&
+                       C.v0s * C.xr < 1e4 && fabs(C.rt) < 700.0 && t < 1e3;
+        if (bates) regular = regular && fabs(p[6] + 0.5 * p[7] * p[7]) < 50.0 && fabs(lt) * (comp + 1.0) < 1e4;
+        if (regular) {
+            C.lnm_re = -C.rt;
+        } else {
+            const Cx phi_mi{0.0, -1.0};
+            Cx m = stable_cf_ref(phi_mi, t, r, v0, kappa, theta, sigma, rho);
+            if (bates) m = cmul(m, jump_cf_ref(phi_mi, t, p[5], p[6], p[7]));
+            Cx lm = clog(m);
+            C.lnm_re = -lm.re;
+            C.lnm_im = -lm.im;
+        }
     }
     C.z0re = -C.rt * C.phi_im + C.lnm_re;
     C.z0im = C.lnm_im;
