@@ -52,7 +52,7 @@ def test_reference_normaliser_is_exp_rt_in_the_regular_region(bates):
         jumps = [rng.uniform(0.0, 5.0), rng.uniform(-0.5, 0.3), rng.uniform(0.01, 0.6)] if bates else None
         cf = O.stable_cf(complex(0.0, -1.0), t, r, hp)
         if bates:
-            cf = cf * O.jump_cf(complex(0.0, -1.0), t, jumps)
+            cf = cf * O.jump_cf(complex(0.0, -1.0), t, hp + jumps)  # a full Bates parameter vector
         finite = math.isfinite(cf.real) and math.isfinite(cf.imag) and cf != 0
         xr = hp[1] - hp[3 + 1] * hp[3]
         if _regular(hp, t, r, jumps):
