@@ -19,8 +19,9 @@
 // Launch shape of the pricing kernel: warps per block and, per model, the
 // minimum resident blocks per SM handed to __launch_bounds__ (which caps
 // registers per thread at 65536 / (32 * WARPS * MINB)): 64 registers x 8
-// blocks for Bates, 72 x 7 for Heston, each the fastest of 6/7/8 blocks on
-// its model's full batch (within 2 % of one another).
+// blocks for both models, the fastest of 5-8 blocks on each model's full
+// batch (within 2 % of one another; kept per model because the optimum has
+// moved apart and back with changes to the node evaluation).
 #ifndef OPE_KERNEL_WARPS
 #define OPE_KERNEL_WARPS 4
 #endif
@@ -28,7 +29,7 @@
 #define OPE_KERNEL_MINB_BATES 8
 #endif
 #ifndef OPE_KERNEL_MINB_HESTON
-#define OPE_KERNEL_MINB_HESTON 7
+#define OPE_KERNEL_MINB_HESTON 8
 #endif
 
 namespace ope {
