@@ -93,3 +93,28 @@ def test_gradient_puts_equal_calls(ope):  # ad.rs:726-729: parity terms do not d
     con["opt_type"] = [0, 1]
     _, g = ope.price_gradient_surfaces(ope.MODEL_BATES, con, [0, 2], np.array([B_REF]), tol=1e-10)
     assert np.array_equal(g[0], g[1])
+
+
+def test_long_integrals_split_into_chunks_match_forward_ad(ope, oracle):
+    """The backward pass splits an integral's stored panels into chunks of 64
+    worked by different warps and adds the chunks' partial sums in order;
+    contracts whose integrals need more than 64 (and more than 128) final
+    panels must match forward-mode AD like any other, alone and inside a
+    batch, and give the same gradient either way."""
+    w = W.c3(n=1 << 14, per_surface=256, seed=9)
+    nb = np.zeros(2 * w.n, np.int32)
+    ope.price_surfaces(ope.MODEL_BATES, w.contracts, w.surf_offsets, w.params, tol=w.tol, bisections=nb)
+    deepest = np.max(nb.reshape(-1, 2), axis=1)
+    pick = np.argsort(-deepest)[:24]
+    assert deepest[pick[0]] >= 128 and deepest[pick[-1]] >= 64, (deepest[pick[0]], deepest[pick[-1]])
+    pick = np.sort(pick)
+    sidx = w.surf_idx()[pick]
+    con = w.contracts[pick]
+    off = np.arange(pick.size + 1, dtype=np.int64)
+    par = w.params[sidx]
+    price, grad = ope.price_gradient_surfaces(ope.MODEL_BATES, con, off, par, tol=w.tol)
+    rp, rg = oracle.batch_price_gradient(con, par, True, w.tol, surf_idx=np.arange(pick.size, dtype=np.int32))
+    _assert_close(grad, rg, what="multi-chunk bates grad")
+    # the same contracts inside their full surfaces
+    _, gfull = ope.price_gradient_surfaces(ope.MODEL_BATES, w.contracts, w.surf_offsets, w.params, tol=w.tol)
+    assert np.array_equal(gfull[pick], grad)
