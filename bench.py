@@ -10,6 +10,10 @@ the persistent multi-surface kernel.  Prints ONE JSON line (rank 0).
   e2e        same metric through the public host API (pinned host buffers,
              H2D of the step's contracts/params/offsets and D2H of prices
              inside the timed region, wall clock around the synchronous call).
+  e2e_pageable  the same from pageable host buffers (what a Rust Vec caller
+             passes): the library copies contracts in and prices out.
+  parity     worst |price - oracle| / S over a sample; above 1e-9 the run
+             prints its line and exits with status 3.
   plain      the reference-shaped drop-in: one batch_bates call per surface
              (host buffers, synchronous), on a sample of surfaces.
   roofline   FP64 bound: algorithmic FP64 ops per launch (ope_b200.roofline)
@@ -20,6 +24,8 @@ the persistent multi-surface kernel.  Prints ONE JSON line (rank 0).
 ``--impl reference`` times that CPU implementation alone (rank 0 only).
 Multi-GPU (torchrun): every rank prices its own 1M-contract shard (weak
 scaling, no collective on the data path); timing is the max over ranks.
+``--gpus N`` without torchrun starts the N ranks itself; under torchrun
+WORLD_SIZE must equal N.
 """
 from __future__ import annotations
 
@@ -44,6 +50,7 @@ import numpy as np  # noqa: E402
 
 METRIC = "Heston/Bates prices/s batched vs plain, 1 B200, ≤1e-9 err; p50/p99 latency"
 UNIT = "contracts/s"
+PARITY_BAR = 1e-9  # max |price - oracle| / S per contract; the run exits 3 above it
 
 
 def parse_args():
@@ -52,7 +59,7 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--n", type=int, default=1 << 20, help="contracts per rank")
+    ap.add_argument("--contracts", type=int, default=1 << 20, help="contracts per rank")
     ap.add_argument("--plain-surfaces", type=int, default=256)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -116,7 +123,7 @@ def run_reference(args) -> None:
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
-    w = workload(args.n, 0)
+    w = workload(args.contracts, 0)
     per_step = max(0.2, min(args.cpu_seconds, 60.0 / max(1, args.steps + args.warmup)))
     for _ in range(args.warmup):
         cpu_sample(w, per_step / 4, rng_seed=17)
@@ -538,6 +545,8 @@ def run_ours(args) -> None:
     from ope_b200 import multi
 
     rank, local_rank, world = multi.rank_info()
+    if torch.cuda.device_count() < world:
+        raise SystemExit(f"bench.py: {world} ranks but {torch.cuda.device_count()} visible GPU(s)")
     torch.cuda.set_device(local_rank)
     dist = multi.init("nccl")
 
@@ -547,7 +556,7 @@ def run_ours(args) -> None:
     def max_over_ranks(x: float) -> float:
         return multi.max_over_ranks(dist, x, device="cuda")
 
-    w = workload(args.n, rank)
+    w = workload(args.contracts, rank)
     n, n_surf = w.n, w.n_surf
     model = ope.MODEL_BATES
     dev = torch.device("cuda", local_rank)
@@ -628,6 +637,21 @@ def run_ours(args) -> None:
     h2d = n * 56 + (n_surf + 1) * 8 + n_surf * 8 * 8
     d2h = n * 8
 
+    # e2e from pageable host buffers (a Rust Vec): the library stages the
+    # contracts into device memory and copies the prices back around the launch
+    pg_out = np.empty(n)
+    ope.price_surfaces(model, w.contracts, w.surf_offsets, w.params, tol=w.tol, out=pg_out)
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        ope.price_surfaces(model, w.contracts, w.surf_offsets, w.params, tol=w.tol, out=pg_out)
+    pageable_s = max_over_ranks(time.perf_counter() - t0)
+    pageable_value = multi.weak_scaling_value(world, n, args.steps, pageable_s)
+    assert np.array_equal(pg_out, ref_prices), "pageable-buffer prices differ from the device-path prices"
+
     # the plain drop-in: one synchronous batch_bates call per surface (host buffers)
     rng = np.random.default_rng(1000 + rank)
     picks = np.sort(rng.choice(n_surf, min(args.plain_surfaces, n_surf), replace=False))
@@ -658,6 +682,9 @@ def run_ours(args) -> None:
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "api": "ope_price_surfaces (host pointers, pinned: the kernel reads the contracts and writes the prices "
                        "in place over PCIe, zero-copy)"},
+        "e2e_pageable": {"value": pageable_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                         "api": "ope_price_surfaces (host pointers, pageable: contracts copied to device memory before "
+                                "the launch, prices copied back after it)"},
         "plain": {"value": plain_value, "unit": UNIT, "surfaces_sampled": int(picks.size),
                   "api": "ope_batch_bates per surface (host pointers, synchronous)",
                   "batched_e2e_over_plain": e2e_value / plain_value,
@@ -695,10 +722,40 @@ def run_ours(args) -> None:
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
+    worst = line.get("parity", {}).get("max_abs_err_over_spot", 0.0)
+    if not worst <= PARITY_BAR:
+        print(f"bench.py: parity breach: max |gpu - oracle| / S = {worst:.3e} > {PARITY_BAR:g}", file=sys.stderr)
+        sys.exit(3)
+
+
+def ranks_or_relaunch(args) -> int | None:
+    """--gpus N means N ranks, one per GPU.  Under torchrun WORLD_SIZE must be
+    N (else exit 2).  Started without torchrun and N > 1, bench.py starts the N
+    ranks itself through torch.distributed.run (rendezvous on 127.0.0.1) and
+    returns that run's exit status; None: carry on in this process."""
+    env_world = os.environ.get("WORLD_SIZE")
+    if env_world is not None:
+        if int(env_world) != args.gpus:
+            print(f"bench.py: --gpus {args.gpus} but WORLD_SIZE={env_world}: run one rank per GPU", file=sys.stderr)
+            return 2
+        return None
+    if args.gpus <= 1:
+        return None
+    import socket
+
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+           "--master-addr", "127.0.0.1", f"--master-port={port}", os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
 
 
 def main():
     args = parse_args()
+    rc = ranks_or_relaunch(args)
+    if rc is not None:
+        sys.exit(rc)
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -334,21 +334,41 @@ int ope_price_surfaces_stats(int32_t model, const ope_contract* contracts, size_
 int ope_measure_fp64_peak(double* flops_per_s, double* elapsed_ms);
 
 /* No counterpart in the reference.  For callers that cannot let a library
- * allocate device memory -- pricing under stream capture (where cudaMalloc is
- * not allowed), latency paths that cannot take cudaMalloc/cudaFree's device
- * synchronisation, hosts whose device memory belongs to another allocator --
- * this is ope_price_surfaces with DEVICE pointers only that allocates nothing:
- * the kernel's scratch lives in a static device array of this library (about
- * 1.25 MiB on every GPU that loads it, held until exit), so n is limited to
- * OPE_NOALLOC_MAX_CONTRACTS (larger n: OPE_ERR_INVALID_ARG).  Stream-ordered
- * on `stream` (cudaStream_t, NULL = legacy default stream).  The first call on
- * a device looks up the array's device address; make it before any stream
- * capture.  Every call shares the one array, so calls whose work overlaps on
- * the GPU race: serialise them on one stream (or order them with events). */
+ * allocate device memory: a host that hands all of a GPU's memory to one
+ * allocator (a framework's caching allocator, or a fixed arena sized at
+ * start-up) has none left for a library's own cudaMalloc, and a latency-
+ * critical request path cannot afford cudaMalloc/cudaFree, either of which
+ * may wait for the whole device.  This is ope_price_surfaces with DEVICE
+ * pointers only that allocates nothing: the kernel's scratch lives in a static
+ * device array of this library (about 1.25 MiB on every GPU that loads it,
+ * held until exit), so n is limited to OPE_NOALLOC_MAX_CONTRACTS (larger n:
+ * OPE_ERR_INVALID_ARG).  tol <= 0 selects OPE_REF_TOL; NaN or infinity is
+ * OPE_ERR_INVALID_ARG.  Stream-ordered on `stream` (cudaStream_t, NULL =
+ * legacy default stream).  The first call on a device does the set-up, with
+ * that device current: it looks up the array's device address and sets up
+ * both models' kernels; make that first call before any stream capture.
+ * Every call shares the one array, so calls whose work overlaps on the GPU
+ * race: serialise them on one stream (or order them with events). */
 #define OPE_NOALLOC_MAX_CONTRACTS 65536
 int ope_price_surfaces_noalloc(int32_t model, const ope_contract* d_contracts, size_t n,
                                const int64_t* d_surf_offsets, size_t n_surf, const void* d_params,
                                double* d_out_prices, double tol, void* stream);
+
+/* No reference twin (diagnostic of heston.rs:193-212 adaptive_gk): the step
+ * by step record of the greedy GK15 quadrature on integral `which` (0 = P1,
+ * 1 = P2) of one contract, made by the pricing kernel's own warp routine and
+ * node evaluation.  Host pointers; synchronous.  Per step j (0 = the first
+ * panel [0, 1], j >= 1 = the j-th bisection) OPE_TRACE_FIELDS doubles:
+ * a, b and the error estimate of the bisected panel (0, 1, 0 at j = 0); K and
+ * error estimate of the left and right children (j = 0: the first panel's K
+ * and error, 0, 0); the running error and total after the step; the 15
+ * integrand values of the left child and the 15 of the right child (zeros at
+ * j = 0).  At most min(max_steps, OPE_MAX_PANELS) steps are written;
+ * *out_n_steps receives the number of steps the integral took and
+ * *out_integral the integral.  tol <= 0 selects OPE_REF_TOL. */
+#define OPE_TRACE_FIELDS 39
+int ope_trace_integral(int32_t model, const ope_contract* contract, const void* params, int32_t which, double tol,
+                       double* out_steps, int32_t max_steps, int32_t* out_n_steps, double* out_integral);
 
 /* No reference twin (numerics self-check): the worst error, in ulps, of the
  * kernels' Newton-refined reciprocal and square root against IEEE 1/x and

@@ -263,7 +263,9 @@ template <class K>
 int grad_grid(K kernel, size_t smem, unsigned long long need, int* grid) {
     int per_sm = 0;
     OPE_TRY(blocks_per_sm(reinterpret_cast<const void*>(kernel), 128, smem, &per_sm));
-    const int cap = std::max(1, (int)(per_sm * tctx().sm_count * tctx().grid_fraction));
+    int sms = 0;
+    OPE_TRY(current_device_sms(&sms));
+    const int cap = std::max(1, (int)(per_sm * sms * tctx().grid_fraction));
     *grid = (int)std::min<unsigned long long>((unsigned long long)cap, need);
     return OPE_OK;
 }

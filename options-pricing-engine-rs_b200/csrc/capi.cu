@@ -88,31 +88,50 @@ int ensure_workspace(size_t bytes, void** out, cudaStream_t st) {
         return set_error(OPE_ERR_OUT_OF_MEMORY, "call needs " + std::to_string(bytes) +
                                                     " bytes of device workspace, above this thread's limit of " +
                                                     std::to_string(c.ws_limit) + " (ope_set_workspace_limit)");
+    // order st after the previous call's use of the workspace (another stream)
+    if (c.ws_recorded && c.ws_stream != st) OPE_CHECK(cudaStreamWaitEvent(st, c.ws_event, 0));
     if (bytes > c.ws_bytes) {
-        if (c.ws) {
-            OPE_CHECK(cudaDeviceSynchronize());
-            OPE_CHECK(cudaFree(c.ws));
-            c.ws = nullptr;
-            c.ws_bytes = 0;
-            c.ws_recorded = false;  // nothing in flight uses the old one
-        }
         size_t want = std::max(bytes, c.ws_bytes + c.ws_bytes / 2);
         want = align_up(want, 1 << 20);
         if (c.ws_limit) want = std::max(bytes, std::min(want, c.ws_limit));
-        OPE_CHECK(cudaMalloc(&c.ws, want));
+        // Stream-ordered: the old block is freed on st after every earlier use
+        // of it (they are all ordered before st by the wait above, or were
+        // enqueued on st by this call), and the new block is valid for work
+        // enqueued on st from here on.  Neither call synchronises the device,
+        // so growing one thread's workspace never stalls other streams.
+        if (c.ws) {
+            OPE_CHECK(cudaFreeAsync(c.ws, st));
+            c.ws = nullptr;
+            c.ws_bytes = 0;
+        }
+        OPE_CHECK(cudaMallocAsync(&c.ws, want, st));
         c.ws_bytes = want;
     }
-    if (c.ws_recorded && c.ws_stream != st) OPE_CHECK(cudaStreamWaitEvent(st, c.ws_event, 0));
     c.ws_stream = st;
     c.ws_taken = true;
     *out = c.ws;
     return OPE_OK;
 }
 
+int current_device_sms(int* sms) {
+    constexpr int kMaxDevices = 64;
+    static std::mutex mu;
+    static int cache[kMaxDevices] = {};
+    int dev = -1;
+    OPE_CHECK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return set_error(OPE_ERR_NO_DEVICE, "device index out of range");
+    std::lock_guard<std::mutex> g(mu);
+    if (cache[dev] == 0) OPE_CHECK(cudaDeviceGetAttribute(&cache[dev], cudaDevAttrMultiProcessorCount, dev));
+    *sms = cache[dev];
+    return OPE_OK;
+}
+
 int blocks_per_sm(const void* kernel, int threads, size_t smem, int* per_sm) {
     static std::mutex mu;
     static std::map<std::tuple<const void*, int, int, size_t>, int> cache;
-    const auto key = std::make_tuple(kernel, tctx().device, threads, smem);
+    int dev = -1;
+    OPE_CHECK(cudaGetDevice(&dev));
+    const auto key = std::make_tuple(kernel, dev, threads, smem);
     {
         std::lock_guard<std::mutex> g(mu);
         const auto it = cache.find(key);
@@ -291,10 +310,14 @@ int ope_set_workspace_limit(uint64_t bytes) {
     ThreadCtx& c = tctx();
     c.ws_limit = (size_t)bytes;
     if (bytes && c.ws && c.ws_bytes > bytes) {  // give back a workspace above the new cap
-        OPE_CHECK(cudaDeviceSynchronize());
-        OPE_CHECK(cudaFree(c.ws));
+        // stream-ordered after the workspace's last use (its event), on this
+        // thread's own stream (created with the workspace's device)
+        if (c.ws_recorded) OPE_CHECK(cudaStreamWaitEvent(c.stream, c.ws_event, 0));
+        OPE_CHECK(cudaFreeAsync(c.ws, c.stream));
         c.ws = nullptr;
         c.ws_bytes = 0;
+        c.ws_recorded = false;
+        c.ws_stream = nullptr;
     }
     return OPE_OK;
 }

@@ -45,13 +45,23 @@ int check_cuda(cudaError_t e, const char* what);
 int ensure_device();                               // OPE_OK or OPE_ERR_NO_DEVICE
 // The per-thread device workspace, grown to `bytes`, for work enqueued on
 // `st`.  If the previous call of this thread used it on another stream, `st`
-// first waits (on the device) for that call's work.
+// first waits (on the device) for that call's work.  Growth is stream-ordered
+// (cudaFreeAsync of the old block and cudaMallocAsync of the new one on
+// `st`), so it never waits for, or stalls, work on other streams.
 int ensure_workspace(size_t bytes, void** out, cudaStream_t st);
 int ensure_pinned(size_t bytes, void** out);       // grows the pinned staging buffer
 // Resident blocks per SM of `kernel` (threads per block, dynamic shared
 // memory) on the current device, with its dynamic-shared-memory attribute
 // set; queried once per kernel and device, then cached.
 int blocks_per_sm(const void* kernel, int threads, size_t smem, int* per_sm);
+// SM count of the current device (queried once per device, then cached).
+// Persistent grids are sized from it, so a launch is sized for the device it
+// runs on whichever thread makes it.
+int current_device_sms(int* sms);
+// Sets up both models' plain pricing kernels on the current device (their
+// shared-memory attribute and occupancy query), so that later launches of
+// them make no CUDA runtime calls besides the launch and its memset.
+int prepare_price_kernels();
 
 // Profiler ranges (NVTX, header-only: free when no tool is attached), one
 // per C-ABI call and per server micro-batch.

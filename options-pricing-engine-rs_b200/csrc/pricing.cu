@@ -185,9 +185,10 @@ __global__ void __launch_bounds__(OPE_KERNEL_WARPS * 32, BATES ? OPE_KERNEL_MINB
 
 template <class K>
 int persistent_grid(K kernel, int threads, size_t smem, int* grid) {
-    int per_sm = 0;
+    int per_sm = 0, sms = 0;
     OPE_TRY(blocks_per_sm(reinterpret_cast<const void*>(kernel), threads, smem, &per_sm));
-    *grid = std::max(1, (int)(per_sm * tctx().sm_count * tctx().grid_fraction));
+    OPE_TRY(current_device_sms(&sms));
+    *grid = std::max(1, (int)(per_sm * sms * tctx().grid_fraction));
     return OPE_OK;
 }
 
@@ -209,6 +210,15 @@ int launch_impl(const ope_contract* con, size_t n, const int64_t* surf_offsets, 
 }
 
 }  // namespace
+
+int prepare_price_kernels() {
+    const int threads = OPE_KERNEL_WARPS * 32;
+    const size_t smem = OPE_KERNEL_WARPS * sizeof(PanelStore);
+    int grid = 0;
+    OPE_TRY(persistent_grid(k_price_persistent<false, false>, threads, smem, &grid));
+    OPE_TRY(persistent_grid(k_price_persistent<true, false>, threads, smem, &grid));
+    return OPE_OK;
+}
 
 int launch_price_persistent(int model, const ope_contract* con, size_t n, const int64_t* surf_offsets,
                             size_t n_surf, const int32_t* param_idx, const double* params, double tol, double* out,

@@ -116,14 +116,27 @@ __device__ __forceinline__ void gk_sums(double f, const LaneRule& R, double& Kl,
     Gr = __shfl_sync(FULL, v, 24);
 }
 
+// Step hooks of gk_integrate_warp.  The pricing kernels use NoTrace (empty
+// and inlined: no code); the QAG trace kernel (trace.cu) records every step.
+//   first(lane, f, k0, e0): the first panel [0, 1] (f: this lane's integrand
+//     value, lanes 0-14 hold the 15 nodes);
+//   step(j, lane, f, a, b, ew, kl, el, kr, er, err, total): bisection j of
+//     panel [a, b] (error estimate ew) into children with K and error
+//     estimates kl, el, kr, er, and the running error and total after it.
+struct NoTrace {
+    __device__ __forceinline__ void first(int, double, double, double) const {}
+    __device__ __forceinline__ void step(int, int, double, double, double, double, double, double, double, double,
+                                         double, double) const {}
+};
+
 // Returns the integral (identical in every lane).  `nbis` receives the
 // number of bisections (loop iterations of heston.rs:200-210); the final
 // live-panel list (nbis + 1 entries) is left in L.  The first panel and every
 // bisection go through ONE call site of the integrand, so the (large) inlined
 // node evaluation exists once in the instruction stream.
-template <bool BATES>
+template <bool BATES, class Trace = NoTrace>
 __device__ __forceinline__ double gk_integrate_warp(const CfConsts& C, double tol, PanelStore& L, int lane,
-                                                    const LaneRule& R, int* nbis) {
+                                                    const LaneRule& R, int* nbis, const Trace& tr = Trace()) {
     const unsigned FULL = 0xffffffffu;
     double total = 0.0, err = 0.0;
     int len = 0;
@@ -148,12 +161,14 @@ __device__ __forceinline__ double gk_integrate_warp(const CfConsts& C, double to
             total = k0;
             err = e0;
             len = 1;
+            tr.first(lane, f, k0, e0);
         } else {
             const double hl = 0.5 * (m - aw), hr = 0.5 * (bw - m);
             const double kl = __dmul_rn(Kl, hl), el = __dmul_rn(fabs(Kl - Gl), hl);
             const double kr = __dmul_rn(Kr, hr), er = __dmul_rn(fabs(Kr - Gr), hr);
             total = __dadd_rn(total, __dsub_rn(__dadd_rn(kl, kr), kw));
             err = __dadd_rn(err, __dsub_rn(__dadd_rn(el, er), ew));
+            tr.step(len, lane, f, aw, bw, ew, kl, el, kr, er, err, total);
             if (lane == 0) {
                 const int last = len - 1;
                 if (w != last) {  // swap_remove

@@ -99,6 +99,7 @@ _sig("ope_server_cancel", ctypes.c_int, [_vp, _u64])
 _sig("ope_server_get_stats", ctypes.c_int, [_vp, _vp])
 _sig("ope_price_surfaces_noalloc", ctypes.c_int, [_i32, _vp, _sz, _vp, _sz, _vp, _vp, _d, _vp])
 _sig("ope_measure_fp64_peak", ctypes.c_int, [ctypes.POINTER(_d), ctypes.POINTER(_d)])
+_sig("ope_trace_integral", ctypes.c_int, [_i32, _vp, _vp, _i32, _d, _vp, _i32, ctypes.POINTER(_i32), ctypes.POINTER(_d)])
 
 _lib = None
 

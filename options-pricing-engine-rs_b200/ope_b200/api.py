@@ -490,6 +490,31 @@ def measure_fp64_peak() -> tuple[float, float]:
     return f.value, ms.value
 
 
+TRACE_FIELDS = 39  # OPE_TRACE_FIELDS
+MAX_STEPS = 200    # OPE_MAX_PANELS: the first panel + at most 199 bisections
+
+
+def trace_integral(model: int, contract, params, which: int, tol=REF_TOL):
+    """Step-by-step record of the device's greedy GK15 quadrature
+    (heston.rs:193-212) on integral `which` (0 = P1, 1 = P2) of one contract:
+    a (steps, TRACE_FIELDS) array -- per step a, b, ew of the bisected panel,
+    kl, el, kr, er of its children, the running error and total, then the 15
+    left and 15 right integrand values -- and the integral."""
+    if isinstance(contract, np.void):
+        contract = np.array([contract], dtype=CONTRACT_DTYPE)
+    elif not isinstance(contract, np.ndarray):
+        contract = [contract]
+    con = contracts_array(contract)
+    if con.size != 1:
+        raise ValueError("trace_integral takes one contract")
+    par = _params_array(params, model)
+    out = np.zeros((MAX_STEPS, TRACE_FIELDS))
+    n, integral = ctypes.c_int32(), ctypes.c_double()
+    check(load().ope_trace_integral(model, con.ctypes.data, par.ctypes.data, int(which), float(tol), out.ctypes.data,
+                                    MAX_STEPS, ctypes.byref(n), ctypes.byref(integral)))
+    return out[:n.value], integral.value
+
+
 # ---------------------------------------------------------------- device path
 def _torch_stream_ptr() -> int:
     import torch
@@ -555,5 +580,5 @@ __all__ = [
     "MULTISTART_RESULT_DTYPE", "GLOBAL_RESULT_DTYPE", "calibrate_surfaces_reg", "calibrate_multistart",
     "calibrate_global", "calibrate_heston_regularized", "calibrate_bates_regularized", "calibrate_heston_multistart",
     "calibrate_bates_multistart", "calibrate_heston_global", "calibrate_bates_global",
-    "calibrate_heston_global_regularized", "calibrate_bates_global_regularized",
+    "calibrate_heston_global_regularized", "calibrate_bates_global_regularized", "trace_integral",
 ]

@@ -163,9 +163,10 @@ inline Cx jump_cf(Cx phi, double t, const Bates& bp) {
     return cexp((lambda * t) * ((jump - 1.0) - (I * phi) * comp));
 }
 
-// heston.rs:180-187
+// heston.rs:180-187.  fv_out (optional): the 15 integrand values, for the
+// step trace below.
 template <class F>
-inline void gk15_panel(const F& f, double a, double b, double* k_out, double* e_out) {
+inline void gk15_panel(const F& f, double a, double b, double* k_out, double* e_out, double* fv_out = nullptr) {
     double c = 0.5 * (a + b);
     double h = 0.5 * (b - a);
     double fv[15];
@@ -176,7 +177,35 @@ inline void gk15_panel(const F& f, double a, double b, double* k_out, double* e_
     for (int j = 0; j < 7; ++j) g = g + G7_WEIGHTS[j] * fv[G7_IDX[j]];
     *k_out = k * h;
     *e_out = std::fabs(k - g) * h;
+    if (fv_out) std::memcpy(fv_out, fv, sizeof(fv));
 }
+
+// Step record of adaptive_gk (a diagnostic of the greedy QAG's decisions,
+// field for field what the device library's ope_trace_integral records):
+// per step j (0 = the first panel [0, 1], j >= 1 = the j-th bisection)
+// TRACE_FIELDS doubles: the bisected panel a, b and its error estimate
+// (0, 1, 0 at j = 0), the children's K and error estimates kl, el, kr, er
+// (j = 0: the first panel's K, err, 0, 0), the running error and total after
+// the step, then the 15 integrand values of the left child and the 15 of the
+// right child (j = 0: the first panel's 15, then zeros).
+constexpr int TRACE_FIELDS = 39;
+struct QagTrace {
+    double* out;
+    int max_steps;
+    int steps = 0;
+    void record(int j, double a, double b, double ew, double kl, double el, double kr, double er, double err,
+                double total, const double* fl, const double* fr) {
+        steps = j + 1;
+        if (j >= max_steps) return;
+        double* r = out + (size_t)j * TRACE_FIELDS;
+        const double head[9] = {a, b, ew, kl, el, kr, er, err, total};
+        std::memcpy(r, head, sizeof(head));
+        for (int i = 0; i < 15; ++i) {
+            r[9 + i] = fl[i];
+            r[24 + i] = fr ? fr[i] : 0.0;
+        }
+    }
+};
 
 // f64::total_cmp key (Rust core::f64::total_cmp)
 inline int64_t total_key(double x) {
@@ -190,15 +219,17 @@ struct Panel { double err, k, a, b; };
 
 // heston.rs:193-212.  `bisections` (optional) counts loop iterations.
 template <class F>
-inline double adaptive_gk(const F& f, double a, double b, double tol, int* bisections) {
+inline double adaptive_gk(const F& f, double a, double b, double tol, int* bisections, QagTrace* tr = nullptr) {
     double k0, e0;
-    gk15_panel(f, a, b, &k0, &e0);
+    double fl[15], fr[15];
+    gk15_panel(f, a, b, &k0, &e0, tr ? fl : nullptr);
     Panel panels[MAX_PANELS + 1];
     int len = 0;
     panels[len++] = Panel{e0, k0, a, b};
     double total = k0;
     double err = e0;
     int nb = 0;
+    if (tr) tr->record(0, a, b, 0.0, k0, e0, 0.0, 0.0, err, total, fl, nullptr);
     while (err > tol && len < MAX_PANELS) {
         // (0..len).max_by(total_cmp): the LAST maximum wins ties
         int w = 0;
@@ -212,13 +243,14 @@ inline double adaptive_gk(const F& f, double a, double b, double tol, int* bisec
         --len;
         double m = 0.5 * (pw.a + pw.b);
         double kl, el, kr, er;
-        gk15_panel(f, pw.a, m, &kl, &el);
-        gk15_panel(f, m, pw.b, &kr, &er);
+        gk15_panel(f, pw.a, m, &kl, &el, tr ? fl : nullptr);
+        gk15_panel(f, m, pw.b, &kr, &er, tr ? fr : nullptr);
         total += (kl + kr) - pw.k;
         err += (el + er) - pw.err;
         panels[len++] = Panel{el, kl, pw.a, m};
         panels[len++] = Panel{er, kr, m, pw.b};
         ++nb;
+        if (tr) tr->record(nb, pw.a, pw.b, pw.err, kl, el, kr, er, err, total, fl, fr);
     }
     if (bisections) *bisections = nb;
     return total;
@@ -226,7 +258,7 @@ inline double adaptive_gk(const F& f, double a, double b, double tol, int* bisec
 
 // heston.rs:220-229 (tol made a parameter; the reference hard-codes 1e-8)
 template <class F>
-inline double gk_integrate(const F& f, double tol, int* bisections) {
+inline double gk_integrate(const F& f, double tol, int* bisections, QagTrace* tr = nullptr) {
     auto g = [&](double t) -> double {
         if (t <= 0.0) return 0.0;
         double u = (1.0 - t) / t;
@@ -234,7 +266,7 @@ inline double gk_integrate(const F& f, double tol, int* bisections) {
         double v = f(u) / (t * t);
         return std::isfinite(v) ? v : 0.0;
     };
-    return adaptive_gk(g, 0.0, 1.0, tol, bisections);
+    return adaptive_gk(g, 0.0, 1.0, tol, bisections, tr);
 }
 
 // heston.rs:101-109
@@ -1270,6 +1302,34 @@ double orc_heston_price(double spot, double strike, double expiry, double rate, 
 double orc_bates_price(double spot, double strike, double expiry, double rate, double div_yield,
                        const double* bp, int opt_type, double tol, int* bisections2) {
     return bates_price(spot, strike, expiry, rate, div_yield, bates_from(bp), opt_type, tol, bisections2);
+}
+
+// Step trace of one Gil-Pelaez integral (which: 0 = P1, 1 = P2) of one
+// contract, with the integrand built as heston_call / bates_call build it
+// (heston.rs:86-93, bates.rs:53-59).  out: max_steps x TRACE_FIELDS doubles
+// (QagTrace).  Returns the number of steps (1 + bisections); *integral
+// receives the integral.
+int orc_trace_integral(const void* contract, const double* params, int bates, int which, double tol,
+                       double* out, int max_steps, double* integral) {
+    const Contract& c = *static_cast<const Contract*>(contract);
+    const double x = std::log(c.spot / c.strike);
+    const double t = c.expiry, r = c.rate;
+    QagTrace tr{out, max_steps};
+    double v;
+    if (bates) {
+        const Bates bp = bates_from(params);
+        const Cx phi_mi{0.0, -1.0};
+        const Cx cf_mi = stable_cf(phi_mi, t, r, bp.h) * jump_cf(phi_mi, t, bp);
+        v = gk_integrate([&](double u) { return bates_integrand(u, x, t, r, bp, which == 0, which == 0 ? &cf_mi : nullptr); },
+                         tol, nullptr, &tr);
+    } else {
+        const Heston p = heston_from(params);
+        const Cx cf_mi = stable_cf(Cx{0.0, -1.0}, t, r, p);
+        v = gk_integrate([&](double u) { return cf_integrand(u, x, t, r, p, which == 0, which == 0 ? &cf_mi : nullptr); },
+                         tol, nullptr, &tr);
+    }
+    if (integral) *integral = v;
+    return tr.steps;
 }
 
 // batch.rs:23-27 / 38-42 generalised to many parameter sets: contract i uses

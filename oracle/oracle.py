@@ -88,6 +88,7 @@ def lib() -> ctypes.CDLL:
             "orc_heston_price": (d, [d, d, d, d, d, dp, i, d, ip]),
             "orc_bates_price": (d, [d, d, d, d, d, dp, i, d, ip]),
             "orc_batch_price": (None, [vp, i64, ip, dp, i, d, dp, ip, i]),
+            "orc_trace_integral": (i, [vp, dp, i, i, d, dp, i, dp]),
             "orc_batch_greeks": (None, [vp, i64, dp, i, d, dp, i]),
             "orc_npdf": (d, [d]),
             "orc_ncdf": (d, [d]),
@@ -201,6 +202,23 @@ def batch_price(con: np.ndarray, params: np.ndarray, bates: bool, tol: float = R
     lib().orc_batch_price(con.ctypes.data, n, _iptr(si), _dptr(params), int(bates), tol, _dptr(out),
                           _iptr(nb), int(nthreads))
     return (out, nb) if stats else out
+
+
+TRACE_FIELDS = 39  # per step: a, b, ew, kl, el, kr, er, err, total, 15 left + 15 right integrand values
+MAX_STEPS = 200     # the first panel + at most 199 bisections (heston.rs:194)
+
+
+def trace_integral(c, params, bates: bool, which: int, tol: float = REF_TOL):
+    """Step-by-step record of adaptive_gk (heston.rs:193-212) on integral
+    `which` (0 = P1, 1 = P2) of contract `c`: a (steps, TRACE_FIELDS) array
+    and the integral.  Same fields as the device library's trace."""
+    c = np.ascontiguousarray(np.atleast_1d(c), dtype=CONTRACT_DTYPE)
+    params = np.ascontiguousarray(params, dtype=np.float64)
+    out = np.zeros((MAX_STEPS, TRACE_FIELDS))
+    integral = np.zeros(1)
+    n = lib().orc_trace_integral(c.ctypes.data, _dptr(params), int(bates), int(which), tol, _dptr(out), MAX_STEPS,
+                                 _dptr(integral))
+    return out[:n], float(integral[0])
 
 
 def batch_greeks(con: np.ndarray, params, bates: bool, tol: float = REF_TOL, nthreads: int = 0) -> np.ndarray:

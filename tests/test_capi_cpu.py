@@ -1,5 +1,6 @@
 """CPU: the C-ABI library loads, exports every symbol include/ope.h declares,
-and refuses to compute without a device (no CPU fallback)."""
+and refuses to compute without a device (no CPU fallback).  One GPU test:
+the library runs as sm_100a code on the device."""
 import os
 
 import numpy as np
@@ -33,12 +34,15 @@ def test_record_layouts_match_header():
     assert list(CONTRACT_DTYPE.names) == ["spot", "strike", "expiry", "rate", "div_yield", "vol", "opt_type", "pad"]
 
 
-def test_library_is_sm100a_only():
-    import subprocess
-
-    so = os.path.join(ROOT, "options-pricing-engine-rs_b200", "lib", "libope_b200.so")
-    out = subprocess.run(["cuobjdump", "--list-elf", so], capture_output=True, text=True).stdout
-    assert "sm_100a" in out
+@pytest.mark.gpu
+def test_library_runs_on_sm100a(ope):
+    """The library carries sm_100a code only: on the device it reports compute
+    capability 10.0 and its pricing kernel launches and prices."""
+    sms, major, minor = ope.device_info()
+    assert (major, minor) == (10, 0) and sms > 0
+    launches = ope.kernel_launch_count()
+    assert ope.heston_price(100.0, 100.0, 1.0, 0.03, 0.0, [0.04, 2.0, 0.04, 0.3, -0.7]) > 0.0
+    assert ope.kernel_launch_count() == launches + 1
 
 
 @pytest.mark.skipif(HAS_GPU, reason="checks the no-device error path")

@@ -60,7 +60,7 @@ def test_reference_arm_prints_one_json_line():
     import json
 
     p = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "2",
-                        "--warmup", "1", "--n", "8192", "--cpu-seconds", "0.3"], capture_output=True, text=True,
+                        "--warmup", "1", "--contracts", "8192", "--cpu-seconds", "0.3"], capture_output=True, text=True,
                        timeout=300)
     assert p.returncode == 0, p.stderr
     lines = [ln for ln in p.stdout.splitlines() if ln.strip()]
@@ -68,3 +68,26 @@ def test_reference_arm_prints_one_json_line():
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["unit"] == "contracts/s" and d["value"] > 0
     assert d["cpu_baseline"]["kind"] == "port" and d["e2e"]["h2d_bytes_per_step"] == 0
+
+
+def test_gpus_flag_must_match_world_size():
+    env = dict(os.environ, RANK="0", LOCAL_RANK="0", WORLD_SIZE="3")
+    p = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+                        "--warmup", "1", "--gpus", "2"], capture_output=True, text=True, env=env, timeout=120)
+    assert p.returncode == 2 and "WORLD_SIZE=3" in p.stderr and p.stdout.strip() == ""
+
+
+def test_gpus_flag_starts_the_ranks_itself():
+    """--gpus 2 without torchrun: bench.py launches two ranks (torch.distributed.run);
+    the reference arm's rank 0 prints one line for the 2-rank job, rank 1 nothing."""
+    import json
+
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "LOCAL_RANK", "WORLD_SIZE", "MASTER_ADDR",
+                                                          "MASTER_PORT")}
+    p = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+                        "--warmup", "1", "--gpus", "2", "--contracts", "4096", "--cpu-seconds", "0.2"],
+                       capture_output=True, text=True, env=env, timeout=300)
+    assert p.returncode == 0, p.stderr[-2000:]
+    lines = [ln for ln in p.stdout.splitlines() if ln.strip().startswith("{")]
+    assert len(lines) == 1
+    assert json.loads(lines[0])["n_gpus"] == 2
