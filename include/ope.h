@@ -387,6 +387,17 @@ int ope_selftest_atan2(uint64_t* max_ulp);
  * and around 1. */
 int ope_selftest_log(uint64_t* max_ulp);
 
+/* No reference twin (numerics self-check of heston.rs:223, u = (1 - t)/t):
+ * the number of 2^24 node positions t, uniform in (0, 1) and log-uniform down
+ * to 2^-200, at which the kernels' u differs from the IEEE quotient. */
+int ope_selftest_node_u(uint64_t* mismatches);
+
+/* No reference twin (numerics self-check of heston.rs:86, x = ln(S/K)): the
+ * kernels' correctly rounded logarithm, and CUDA's log for comparison, of n
+ * host arguments (n <= 2^26).  The pricing kernels take x from the former, so
+ * that it rounds as the platform libm's log does in the reference. */
+int ope_selftest_log_cr(const double* args, size_t n, double* out_log_cr, double* out_log_cuda);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

@@ -565,6 +565,22 @@ int ope_selftest_log(uint64_t* max_ulp) {
     return selftest_log(max_ulp);
 }
 
+int ope_selftest_node_u(uint64_t* mismatches) {
+    OPE_RANGE("ope.selftest_node_u");
+    if (!mismatches) return set_error(OPE_ERR_INVALID_ARG, "NULL argument");
+    OPE_TRY(ensure_device());
+    return selftest_node_u(mismatches);
+}
+
+int ope_selftest_log_cr(const double* args, size_t n, double* out_log_cr, double* out_log_cuda) {
+    OPE_RANGE("ope.selftest_log_cr");
+    if (n == 0) return OPE_OK;
+    if (!args || !out_log_cr || !out_log_cuda) return set_error(OPE_ERR_INVALID_ARG, "NULL argument");
+    if (n > ((size_t)1 << 26)) return set_error(OPE_ERR_INVALID_ARG, "n above 2^26");
+    OPE_TRY(ensure_device());
+    return selftest_log_cr(args, n, out_log_cr, out_log_cuda);
+}
+
 int ope_measure_fp64_peak(double* flops_per_s, double* elapsed_ms) {
     OPE_RANGE("ope.measure_fp64_peak");
     if (!flops_per_s || !elapsed_ms) return set_error(OPE_ERR_INVALID_ARG, "NULL argument");

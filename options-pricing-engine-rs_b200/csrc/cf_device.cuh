@@ -129,6 +129,89 @@ __device__ __forceinline__ double log_node(double v) {
     return out;
 }
 
+// Error-free transformations (Knuth's TwoSum, Dekker's Fast2Sum, the FMA
+// product residual) and double-double arithmetic, for log_cr below.
+__device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {
+    s = __dadd_rn(a, b);
+    const double bb = __dsub_rn(s, a);
+    e = __dadd_rn(__dsub_rn(a, __dsub_rn(s, bb)), __dsub_rn(b, bb));
+}
+__device__ __forceinline__ void fast_two_sum(double a, double b, double& s, double& e) {  // |a| >= |b|
+    s = __dadd_rn(a, b);
+    e = __dsub_rn(b, __dsub_rn(s, a));
+}
+struct DD {
+    double hi, lo;
+};
+__device__ __forceinline__ DD dd_add(DD a, DD b) {
+    double s, e;
+    two_sum(a.hi, b.hi, s, e);
+    e = __dadd_rn(e, __dadd_rn(a.lo, b.lo));
+    DD r;
+    fast_two_sum(s, e, r.hi, r.lo);
+    return r;
+}
+__device__ __forceinline__ DD dd_mul(DD a, DD b) {
+    const double p = __dmul_rn(a.hi, b.hi);
+    double e = fma(a.hi, b.hi, -p);
+    e = fma(a.hi, b.lo, fma(a.lo, b.hi, e));
+    DD r;
+    fast_two_sum(p, e, r.hi, r.lo);
+    return r;
+}
+
+// ln(v) correctly rounded (to nearest) for positive normal v, other arguments
+// through CUDA's log.  Used once per integral for x = ln(S/K): the integrand's
+// phase u x reaches 1e7 and beyond on short-dated deep-wing contracts, where
+// one ulp of x moves a node value by 1e-9 relative, so x must be the value
+// the reference's own libm log returns -- the correctly rounded one.  Method
+// (the atanh series of the logarithm, in double-double): v = 2^k m with m in
+// [sqrt(1/2), sqrt 2); s = (m - 1)/(m + 1) as a double-double;
+// ln m = 2s + 2s^3/3 + 2s^5/5 + s^7 q(s^2), q(w) = sum_j 2 w^j/(2j + 7)
+// (|s| <= 0.1716, the first three terms in double-double, q in double); plus
+// k ln 2 with ln 2 as a double-double.  The sum carries about 2^-68 relative
+// error, so the final rounding is correct unless ln v lies within that of a
+// rounding midpoint.
+__device__ __forceinline__ double log_cr(double v) {
+    if (!(v >= 0x1p-1022 && v <= 0x1.fffffffffffffp+1023)) return log(v);
+    const int hi = __double2hiint(v), lo = __double2loint(v);
+    const int k = (hi - 0x3FE6A09E) >> 20;  // 0x3FE6A09E: high word of sqrt(1/2)
+    const double m = __hiloint2double(hi - k * 0x100000, lo);
+    const double f = __dsub_rn(m, 1.0);  // exact (Sterbenz)
+    double dh, dl;
+    fast_two_sum(2.0, f, dh, dl);  // m + 1 = 2 + f exactly
+    const double sh = __ddiv_rn(f, dh);
+    const double res = __dsub_rn(fma(-sh, dh, f), __dmul_rn(sh, dl));  // f - sh (dh + dl)
+    DD S;
+    fast_two_sum(sh, __ddiv_rn(res, dh), S.hi, S.lo);
+    const DD W = dd_mul(S, S);
+    const DD S3 = dd_mul(S, W);
+    const DD S5 = dd_mul(S3, W);
+    const double w = W.hi;
+    double q = 0.07407407407407407;
+    q = fma(q, w, 0.08);
+    q = fma(q, w, 0.08695652173913043);
+    q = fma(q, w, 0.09523809523809523);
+    q = fma(q, w, 0.10526315789473684);
+    q = fma(q, w, 0.11764705882352941);
+    q = fma(q, w, 0.13333333333333333);
+    q = fma(q, w, 0.15384615384615385);
+    q = fma(q, w, 0.18181818181818182);
+    q = fma(q, w, 0.2222222222222222);
+    q = fma(q, w, 0.2857142857142857);
+    const double rest = __dmul_rn(__dmul_rn(S5.hi, w), q);
+    DD acc{__dmul_rn(2.0, S.hi), __dmul_rn(2.0, S.lo)};
+    acc = dd_add(acc, dd_mul(S3, DD{0.6666666666666666, 3.700743415417188e-17}));  // 2/3
+    acc = dd_add(acc, dd_mul(S5, DD{0.4, -2.2204460492503132e-17}));               // 2/5
+    acc = dd_add(acc, DD{rest, 0.0});
+    const double kd = (double)k;
+    DD kl;
+    kl.hi = __dmul_rn(kd, 0.6931471805599453);  // ln 2 = 0.6931471805599453 + 2.3190468138462996e-17
+    kl.lo = fma(kd, 2.3190468138462996e-17, fma(kd, 0.6931471805599453, -kl.hi));
+    acc = dd_add(kl, acc);
+    return __dadd_rn(acc.hi, acc.lo);
+}
+
 __device__ __forceinline__ Cx cadd(Cx a, Cx b) { return Cx{a.re + b.re, a.im + b.im}; }
 __device__ __forceinline__ Cx csub(Cx a, Cx b) { return Cx{a.re - b.re, a.im - b.im}; }
 __device__ __forceinline__ Cx cmul(Cx a, Cx b) {
@@ -179,10 +262,10 @@ __device__ __forceinline__ void csqrt_node(double zr, double zi, double& dre, do
 //   xi   = (xr, -rs u)                       xi = kappa - i rho sigma phi, phi = u + i phi_im
 //   z    = xi^2 + (sig2 u^2, sig2s u)       sigma^2 phi(phi+i)
 //   Re Z = kts Re Ch + v0s Re Dh + z0re      z0re = r T + Re(-Log CF(-i)) for P1, 0 for P2
-//   Im Z = kts Im Ch + v0s Im Dh + rtx u + z0im      rtx = r T + ln(S/K)
+//   Im Z = kts Im Ch + v0s Im Dh + r T u + z0im + (x u mod 2 pi)      x = ln(S/K)
 //   Bates: jump = exp(jr0 - hs2 u^2 + i jmu u);  J = (lt Re jump + jre0, lt Im jump - ltc u)
 struct CfConsts {
-    double xr, rs, sig2, sig2s, kts, v0s, t, rtx, z0re, z0im;
+    double xr, rs, sig2, sig2s, kts, v0s, t, z0re, z0im;
     double jr0, hs2, jmu, lt, jre0, ltc;
     // raw values kept for the adjoint chain
     double kappa, phi_im, sgn, rt, x, lnm_re, lnm_im, mu_j, comp;
@@ -233,12 +316,11 @@ __device__ __forceinline__ CfConsts make_consts(double s, double k, double t, do
     C.v0s = v0 / (sigma * sigma);
     C.t = t;
     C.rt = r * t;
-    C.x = log(s / k);
+    C.x = log_cr(s / k);  // heston.rs:86, rounded as the platform libm rounds it
     C.phi_im = (which == 0) ? -1.0 : 0.0;
     C.sgn = (which == 0) ? -1.0 : 1.0;
     C.xr = kappa + C.rs * C.phi_im;
     C.sig2s = C.sig2 * C.sgn;
-    C.rtx = C.rt + C.x;
     double lt = 0.0, mu_j = 0.0, hs2 = 0.0, comp = 0.0;
     if (bates) {
         lt = p[5] * t;
@@ -285,12 +367,25 @@ __device__ __forceinline__ CfConsts make_consts(double s, double k, double t, do
     return C;
 }
 
+// u = (1 - t)/t of a node, rounded as heston.rs:223 rounds it (the IEEE
+// quotient): at large u the phase u x makes every ulp of u count.  From
+// y ~ 1/t (= (1 - t) itt with itt ~ 1/((1 - t) t), a few ulps) the quotient
+// u0 = (1 - t) y is within a few ulps; one correction with the exact residual
+// (1 - t) - u0 t (an FMA) lands within about 1e-15 ulp of the true quotient,
+// so its rounding is the IEEE one short of a midpoint that close (checked
+// against IEEE division by ope_selftest_node_u).
+__device__ __forceinline__ double node_u(double omt, double tn, double itt) {
+    const double yt = omt * itt;
+    const double u0 = omt * yt;
+    return fma(fma(-u0, tn, omt), yt, u0);
+}
+
 // gk_integrate's g(t) (heston.rs:221-227) with the merged-exponent integrand.
 template <bool BATES>
 __device__ __forceinline__ double node_value(const CfConsts& C, double tn) {
     const double omt = 1.0 - tn;
     const double itt = rcp_nr(omt * tn);  // 1 / ((1 - t) t)
-    const double u = (omt * omt) * itt;   // (1 - t) / t
+    const double u = node_u(omt, tn, itt);    // (1 - t) / t
     const double u2 = u * u;
     // xi = (xr, xi_) ; z = xi^2 + sigma^2 phi(phi+i)
     const double xr = C.xr, xi_ = -C.rs * u;
@@ -344,8 +439,19 @@ __device__ __forceinline__ double node_value(const CfConsts& C, double tn) {
     // Ch = (xi - d) T - 2 Log A
     const double Cr = fma(amr, C.t, -2.0 * lr);
     const double Ci = fma(ami, C.t, -2.0 * li);
+    // The phase of e^{iux} (heston.rs:107), u x rounded as the reference
+    // rounds it, reduced modulo 2 pi without loss (Cody and Waite's argument
+    // reduction, 2 pi split into two doubles and the products taken exactly by
+    // FMA: |u x - n 2 pi| < 4 makes the first step exact), so that adding the
+    // CF's own phase costs an ulp of a number below 4 however large u x is.
+    // The reference adds the two phases exactly too, through the complex
+    // product e^{iux} CF (an unreduced sum would lose ulp(u x), 1e-9 at
+    // u x = 1e7, on short-dated deep-wing contracts).
+    const double ux = __dmul_rn(u, C.x);
+    const double nq = rint(ux * 0.15915494309189535);  // 1 / (2 pi)
+    const double uxr = fma(-nq, 2.4492935982947064e-16, fma(-nq, 6.283185307179586, ux));
     double zre = fma(C.kts, Cr, fma(C.v0s, Dr, C.z0re));
-    double zim = fma(C.kts, Ci, fma(C.v0s, Di, fma(C.rtx, u, C.z0im)));
+    double zim = fma(C.kts, Ci, fma(C.v0s, Di, fma(C.rt, u, C.z0im))) + uxr;
     if (BATES) {
         double js, jc;
         sincos(C.jmu * u, &js, &jc);

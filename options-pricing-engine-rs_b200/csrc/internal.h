@@ -189,6 +189,8 @@ int measure_fp64_peak(double* flops, double* ms);
 int selftest_math(uint64_t* ulp_rcp, uint64_t* ulp_sqrt);
 int selftest_atan2(uint64_t* ulp);
 int selftest_log(uint64_t* ulp);
+int selftest_log_cr(const double* v, size_t n, double* out_cr, double* out_cuda);
+int selftest_node_u(uint64_t* mismatches);
 // Bump-and-reprice Greeks (greeks.rs:19-72) for n contracts under one
 // parameter set; `ws` must hold greeks_workspace_bytes(n) bytes.
 size_t greeks_workspace_bytes(size_t n);

@@ -79,7 +79,65 @@ __global__ void k_selftest_log(unsigned long long* ulp) {
     atomicMax(ulp, (unsigned long long)d);
 }
 
+// node_u against IEEE division (1 - t)/t over 2^24 node positions t: uniform
+// in (0, 1), and log-uniform from 2^-200 (the smallest panel 200 bisections
+// can make) to 1/2.  Counts the positions where the two differ.
+__global__ void k_selftest_node_u(unsigned long long* mismatches) {
+    const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long h = 0x9E3779B97F4A7C15ull * (i + 1);
+    h ^= h >> 31;
+    h *= 0xBF58476D1CE4E5B9ull;
+    h ^= h >> 29;
+    const double r = (double)(h >> 11) * 0x1.0p-53;  // [0, 1)
+    const double tn = (i & 1) ? exp2(-200.0 * r - 1.0) : fmax(r, 0x1.0p-53);
+    const double omt = 1.0 - tn;
+    const double u = node_u(omt, tn, rcp_nr(omt * tn));
+    if (u != __ddiv_rn(omt, tn)) atomicAdd(mismatches, 1ull);
+}
+
+// log_cr (x = ln(S/K) of every integral) and CUDA's log on given arguments.
+__global__ void k_eval_log_cr(const double* v, long long n, double* out_cr, double* out_cuda) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out_cr[i] = log_cr(v[i]);
+    out_cuda[i] = log(v[i]);
+}
+
 }  // namespace
+
+int selftest_log_cr(const double* v, size_t n, double* out_cr, double* out_cuda) {
+    ThreadCtx& c = tctx();
+    const size_t b = align_up(n * sizeof(double), 256);
+    void* ws;
+    OPE_TRY(ensure_workspace(3 * b, &ws, c.stream));
+    double* d_v = static_cast<double*>(ws);
+    double* d_cr = reinterpret_cast<double*>(static_cast<char*>(ws) + b);
+    double* d_cu = reinterpret_cast<double*>(static_cast<char*>(ws) + 2 * b);
+    OPE_CHECK(cudaMemcpyAsync(d_v, v, n * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    k_eval_log_cr<<<(unsigned)((n + 255) / 256), 256, 0, c.stream>>>(d_v, (long long)n, d_cr, d_cu);
+    OPE_CHECK(cudaGetLastError());
+    c.launches += 1;
+    OPE_CHECK(cudaMemcpyAsync(out_cr, d_cr, n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    OPE_CHECK(cudaMemcpyAsync(out_cuda, d_cu, n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    OPE_CHECK(cudaStreamSynchronize(c.stream));
+    return OPE_OK;
+}
+
+int selftest_node_u(uint64_t* mismatches) {
+    ThreadCtx& c = tctx();
+    void* ws;
+    OPE_TRY(ensure_workspace(256, &ws, c.stream));
+    unsigned long long* d = static_cast<unsigned long long*>(ws);
+    OPE_CHECK(cudaMemsetAsync(d, 0, sizeof(unsigned long long), c.stream));
+    k_selftest_node_u<<<1 << 16, 256, 0, c.stream>>>(d);
+    OPE_CHECK(cudaGetLastError());
+    c.launches += 1;
+    unsigned long long h = 0;
+    OPE_CHECK(cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, c.stream));
+    OPE_CHECK(cudaStreamSynchronize(c.stream));
+    *mismatches = h;
+    return OPE_OK;
+}
 
 int selftest_log(uint64_t* ulp) {
     ThreadCtx& c = tctx();

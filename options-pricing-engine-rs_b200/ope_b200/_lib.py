@@ -80,6 +80,8 @@ _sig("ope_price_gradient_surfaces", ctypes.c_int,
 _sig("ope_selftest_math", ctypes.c_int, [ctypes.POINTER(_u64), ctypes.POINTER(_u64)])
 _sig("ope_selftest_atan2", ctypes.c_int, [ctypes.POINTER(_u64)])
 _sig("ope_selftest_log", ctypes.c_int, [ctypes.POINTER(_u64)])
+_sig("ope_selftest_log_cr", ctypes.c_int, [_vp, _sz, _vp, _vp])
+_sig("ope_selftest_node_u", ctypes.c_int, [ctypes.POINTER(_u64)])
 _sig("ope_calibrate_surfaces", ctypes.c_int,
      [_i32, _vp, _vp, _vp, _sz, _vp, _sz, _vp, _vp, ctypes.POINTER(Options)])
 _sig("ope_calibrate_surfaces_reg", ctypes.c_int,

@@ -307,6 +307,52 @@ def test_own_log_within_two_ulp_of_cuda(ope):
     assert u.value <= 2, u.value
 
 
+def test_node_u_is_the_ieee_quotient(ope):
+    """u = (1 - t)/t of every node (heston.rs:223) from a reciprocal and one
+    FMA correction equals the IEEE quotient the reference computes, at 2^24
+    node positions down to 2^-200."""
+    import ctypes
+
+    from ope_b200 import _lib
+
+    m = ctypes.c_uint64()
+    _lib.check(_lib.load().ope_selftest_node_u(ctypes.byref(m)))
+    assert m.value == 0, m.value
+
+
+def test_correctly_rounded_log_matches_the_platform_libm(ope):
+    """x = ln(S/K) of every integral comes from the kernels' own correctly
+    rounded log (heston.rs:86 calls the platform libm's log, glibc's here).
+    glibc's log is itself not correctly rounded on about 0.06 % of arguments,
+    so: agreement with math.log on all but 0.2 % of 2^18 arguments spread over
+    the normal range and around 1 (and on every S/K of the benchmark
+    configurations' contracts), and where they differ, the kernels' value is
+    the correctly rounded one (mpmath at 120 bits) and glibc's is one ulp off."""
+    import ctypes
+    import math
+
+    import mpmath as mp
+
+    from ope_b200 import _lib
+
+    rng = np.random.default_rng(5)
+    n = 1 << 18
+    v = np.concatenate([np.exp(rng.uniform(-700.0, 700.0, n // 2)), 1.0 + rng.uniform(-0.3, 0.4, n // 4),
+                        np.exp(rng.uniform(-4.5, 4.5, n // 4))])
+    w1, w3 = W.c1(), W.c3(n=1 << 14, per_surface=256)
+    v = np.concatenate([v, w1.contracts["spot"] / w1.contracts["strike"], w3.contracts["spot"] / w3.contracts["strike"]])
+    cr, cu = np.empty_like(v), np.empty_like(v)
+    _lib.check(_lib.load().ope_selftest_log_cr(v.ctypes.data, v.size, cr.ctypes.data, cu.ctypes.data))
+    ref = np.array([math.log(x) for x in v])
+    diff = np.flatnonzero(cr != ref)
+    print(f"log_cr vs glibc: {diff.size} of {v.size} differ; CUDA's log vs glibc: {np.count_nonzero(cu != ref)}")
+    assert diff.size <= 2e-3 * v.size
+    mp.mp.prec = 120
+    for i in diff:
+        assert cr[i] == float(mp.log(mp.mpf(float(v[i])))), (v[i], cr[i], ref[i])
+        assert abs(cr[i] - ref[i]) == math.ulp(abs(cr[i])) or abs(cr[i] - ref[i]) == math.ulp(abs(ref[i]))
+
+
 def test_pinned_host_buffers_zero_copy_equal_copy_path(ope):
     """Contracts and prices in pinned host memory are read and written in place
     by the kernel (zero-copy); the prices equal the pageable (copy) path's."""

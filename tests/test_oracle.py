@@ -77,6 +77,45 @@ def test_oracle_fixtures_unchanged(oracle):
         assert v == float.fromhex(r["price"])
 
 
+def test_oracle_corner_fixture_unchanged(oracle):
+    """The corner contracts of corner_cap_contracts.json (tol 1e-12, both
+    integrals at the 200-panel cap): the oracle's prices and bisection counts
+    are the committed ones, bit for bit."""
+    from ope_b200 import workloads as W
+
+    with open(os.path.join(GOLD, "corner_cap_contracts.json")) as f:
+        d = json.load(f)
+    for e in d["contracts"]:
+        c = np.zeros(1, W.CONTRACT_DTYPE)
+        for k, v in e["contract"].items():
+            c[k] = float.fromhex(v)
+        c["opt_type"] = e["opt_type"]
+        p = np.array([[float.fromhex(x) for x in e["params"]]])
+        px, nb = oracle.batch_price(c, p, bool(e["bates"]), d["tol"], stats=True)
+        assert px[0] == float.fromhex(e["oracle_price"])
+        assert list(nb) == e["oracle_bisections"]
+
+
+def test_oracle_trace_replays_its_own_quadrature(oracle):
+    """The oracle's step trace of adaptive_gk (heston.rs:193-212) is the
+    quadrature it runs: its last total is the integral, its step count is one
+    more than the bisection count, and replaying its choices rebuilds a panel
+    list whose K values sum to that total."""
+    import qag_trace as Q
+    from ope_b200 import workloads as W
+
+    w = W.c3(n=512, per_surface=256)
+    si = w.surf_idx()
+    for i in (0, 7, 300):
+        nb = oracle.batch_price(w.contracts[i:i + 1], w.params[si[i]:si[i] + 1], True, w.tol, stats=True)[1]
+        for which in (0, 1):
+            tr, integral = oracle.trace_integral(w.contracts[i], w.params[si[i]], True, which, w.tol)
+            assert len(tr) == nb[which] + 1 and tr[-1, Q.TOTAL] == integral
+            live = Q.panels_before(tr, len(tr))
+            assert len(live) == len(tr)
+            assert abs(sum(k for k, _, _ in live.values()) - integral) <= 1e-12 * max(1.0, abs(integral))
+
+
 # ---- heston.rs tests --------------------------------------------------------
 def test_put_call_parity(oracle):  # heston.rs:309-316
     call = oracle.heston_price(100.0, 100.0, 0.5, 0.03, 0.0, H_REF, 0)
