@@ -68,6 +68,7 @@ def parse_args():
     ap.add_argument("--grad-n", type=int, default=1 << 18, help="contracts in the adjoint-gradient section")
     ap.add_argument("--no-serving", action="store_true", help="skip the config-5 serving section")
     ap.add_argument("--serving-rates", default="100,1000,5000,20000")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shape (no ope_autotune)")
     return ap.parse_args()
 
 
@@ -567,6 +568,14 @@ def run_ours(args) -> None:
     flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream()
 
+    # untimed set-up: the launch-shape autotuner (ope_autotune) measures this
+    # device once; every call below uses its table unless --no-autotune
+    tune = None
+    if not args.no_autotune:
+        t0 = time.perf_counter()
+        rows = ope.autotune(model)
+        tune = {"seconds": time.perf_counter() - t0, "table": rows}
+
     # untimed: per-integral bisection counts for the work tally
     nb = np.zeros(2 * n, np.int32)
     ope.price_surfaces(model, w.contracts, w.surf_offsets, w.params, tol=w.tol, bisections=nb)
@@ -655,20 +664,50 @@ def run_ours(args) -> None:
     # the plain drop-in: one synchronous batch_bates call per surface (host buffers)
     rng = np.random.default_rng(1000 + rank)
     picks = np.sort(rng.choice(n_surf, min(args.plain_surfaces, n_surf), replace=False))
-    for s in picks[:8]:
-        ope.batch_bates(w.contracts[w.surf_offsets[s]:w.surf_offsets[s + 1]], w.params[s], tol=w.tol)
-    barrier()
-    t0 = time.perf_counter()
-    cnt = 0
-    call_ms = []
-    for s in picks:
-        c = w.contracts[w.surf_offsets[s]:w.surf_offsets[s + 1]]
-        t1 = time.perf_counter()
-        ope.batch_bates(c, w.params[s], tol=w.tol)
-        call_ms.append(1e3 * (time.perf_counter() - t1))
-        cnt += c.size
-    plain_s = max_over_ranks(time.perf_counter() - t0)
-    plain_value = world * cnt / plain_s
+
+    def plain_run():
+        for s in picks[:8]:
+            ope.batch_bates(w.contracts[w.surf_offsets[s]:w.surf_offsets[s + 1]], w.params[s], tol=w.tol)
+        barrier()
+        t0 = time.perf_counter()
+        cnt, call_ms = 0, []
+        for s in picks:
+            c = w.contracts[w.surf_offsets[s]:w.surf_offsets[s + 1]]
+            t1 = time.perf_counter()
+            ope.batch_bates(c, w.params[s], tol=w.tol)
+            call_ms.append(1e3 * (time.perf_counter() - t1))
+            cnt += c.size
+        return world * cnt / max_over_ranks(time.perf_counter() - t0), call_ms
+
+    # 2,048-contract calls (8 surfaces each, the size of a large serving request)
+    groups = [list(range(8 * g, 8 * g + 8)) for g in range(0, min(64, n_surf // 8))]
+    subs = [w.subset(g) for g in groups]
+
+    def mid_run():
+        for sub in subs[:4]:
+            ope.price_surfaces(model, sub.contracts, sub.surf_offsets, sub.params, tol=w.tol)
+        ms = []
+        for sub in subs:
+            t1 = time.perf_counter()
+            ope.price_surfaces(model, sub.contracts, sub.surf_offsets, sub.params, tol=w.tol)
+            ms.append(1e3 * (time.perf_counter() - t1))
+        return ms
+
+    def pct(ms):
+        return {"p50": float(np.percentile(ms, 50)), "p99": float(np.percentile(ms, 99))}
+
+    plain_value, call_ms = plain_run()
+    mid_ms = mid_run()
+    shapes = None
+    if tune is not None:  # the same calls with the default launch shape
+        ope.set_autotune(False)
+        plain_default, call_ms_default = plain_run()
+        mid_ms_default = mid_run()
+        ope.set_autotune(True)
+        shapes = {"plain_value_default_shape": plain_default,
+                  "latency_ms_per_256_contract_surface_default_shape": pct(call_ms_default),
+                  "latency_ms_per_2048_contract_call": pct(mid_ms),
+                  "latency_ms_per_2048_contract_call_default_shape": pct(mid_ms_default)}
 
     peak_flops, _ = ope.measure_fp64_peak()
     achieved = flops_per_launch / (kern_avg * 1e-3)
@@ -688,8 +727,7 @@ def run_ours(args) -> None:
         "plain": {"value": plain_value, "unit": UNIT, "surfaces_sampled": int(picks.size),
                   "api": "ope_batch_bates per surface (host pointers, synchronous)",
                   "batched_e2e_over_plain": e2e_value / plain_value,
-                  "latency_ms_per_256_contract_surface": {"p50": float(np.percentile(call_ms, 50)),
-                                                          "p99": float(np.percentile(call_ms, 99))}},
+                  "latency_ms_per_256_contract_surface": pct(call_ms)},
         "roofline": {"bound": "fp64", "achieved": achieved / 1e12, "peak": peak_flops / 1e12, "unit": "TFLOP/s",
                      "frac": achieved / peak_flops, "traffic": traffic,
                      "peak_source": "measured DFMA-chain probe on this GPU (ope_measure_fp64_peak)",
@@ -701,6 +739,11 @@ def run_ours(args) -> None:
         "gpu_launches": int(launches),
         "clocks": clk,
     }
+    if tune is not None:
+        tune.update(shapes or {})
+        line["autotune"] = tune
+    else:
+        line["plain"]["latency_ms_per_2048_contract_call"] = pct(mid_ms)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, m, dt, cores, worst = cpu_sample(w, args.cpu_seconds, gpu_prices=ref_prices)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",

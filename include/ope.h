@@ -354,6 +354,49 @@ int ope_price_surfaces_noalloc(int32_t model, const ope_contract* d_contracts, s
                                const int64_t* d_surf_offsets, size_t n_surf, const void* d_params,
                                double* d_out_prices, double tol, void* stream);
 
+/* No counterpart in the reference (its batch calls hand contracts to
+ * rayon's work-stealing pool, batch.rs:23-42): the launch-shape autotuner of
+ * the pricing kernel.  A shape is the persistent grid's warps per block (each
+ * warp integrates one of a contract's two integrals), whether the work queue
+ * takes contracts deepest-first (by |ln(K/S)| / sqrt(v0 T)) or in input
+ * order, and the share of the resident blocks per SM the grid fills.  Every
+ * shape gives bit-identical prices; only the time differs.
+ * ope_autotune measures every candidate shape (1, 2 or 4 warps x order x
+ * occupancy 1 or 1/2) on seeded synthetic batches of each size class (at the
+ * class's geometric interior) on the calling thread's device, keeps per class
+ * the fastest shape if it beats the default (4, input order, 1) by more than
+ * 3 %, installs the table for that device and model in this process, and
+ * writes the OPE_TUNE_CLASSES entries to out_entries (may be NULL).  Takes
+ * about 10 s (about 1 s with OPE_TUNE_QUICK).  Plain pricing calls (ope_batch_*,
+ * ope_price_surfaces, Greeks, the server's reprices) then launch with their
+ * class's shape; calibration passes keep the default shape.
+ * ope_set_autotune(0) returns every call to the default shape (1: the tuned
+ * tables again); ope_get_tune_table reads the current device's table
+ * (*out_tuned = 0: not tuned, the default entries); ope_set_tune_table
+ * installs one. */
+typedef struct {
+    int32_t warps_per_block; /* 1, 2 or 4 */
+    int32_t deepest_first;   /* 1: queue deepest-first, 0: input order */
+    double occupancy;        /* share of the resident blocks per SM, (0, 1] */
+} ope_launch_shape;
+typedef struct {
+    uint64_t max_contracts;  /* the class: calls of at most this many contracts (the last: all larger) */
+    ope_launch_shape shape;  /* the shape calls of this class use */
+    double ms_default;       /* measured kernel time of the default shape on the class's batch */
+    double ms_tuned;         /* measured kernel time of `shape` (ms_default when it is the default) */
+} ope_tune_entry;
+#define OPE_TUNE_CLASSES 16  /* calls of up to 64, 128, 256, ..., 2^20 contracts, and larger */
+#define OPE_TUNE_QUICK 1u    /* ope_autotune flag: measure the classes up to 2^17 contracts only (the
+                              * larger ones keep the default shape) */
+int ope_autotune(int32_t model, uint32_t flags, ope_tune_entry* out_entries);
+int ope_set_autotune(int32_t enabled);
+int ope_get_tune_table(int32_t model, ope_tune_entry* out_entries, int32_t* out_tuned);
+/* Installs OPE_TUNE_CLASSES entries (e.g. a table saved from
+ * ope_get_tune_table in an earlier process) as the current device's tuned
+ * table for `model`; each shape must be valid (1, 2 or 4 warps; 0 or 1;
+ * occupancy in (0, 1]), max_contracts is ignored. */
+int ope_set_tune_table(int32_t model, const ope_tune_entry* entries);
+
 /* No reference twin (diagnostic of heston.rs:193-212 adaptive_gk): the step
  * by step record of the greedy GK15 quadrature on integral `which` (0 = P1,
  * 1 = P2) of one contract, made by the pricing kernel's own warp routine and

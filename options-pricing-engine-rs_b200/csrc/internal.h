@@ -99,13 +99,40 @@ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 // Scratch needed by one pricing launch over n contracts: per-contract integral
 // pair + completion counter, and the work-queue head.
+// With order/bucket/hist set (carve_price_scratch sets them), a launch may
+// queue its contracts deepest-first (LaunchShape::deepest_first); left NULL
+// (the allocation-free entry point) it always uses the natural order.
 struct PriceScratch {
-    double* integ;            // 2n
-    unsigned int* done;       // n   (must be zero before launch)
-    unsigned long long* head; // 1   (must be zero before launch; persistent only)
+    double* integ;                 // 2n
+    unsigned int* done;            // n   (must be zero before launch)
+    unsigned long long* head;      // 1   (must be zero before launch; persistent only)
+    uint32_t* order = nullptr;     // n   queue position -> contract
+    uint32_t* bucket = nullptr;    // n   depth bucket of each contract
+    unsigned int* hist = nullptr;  // 2 x 64 bucket counts and fill counters
 };
 size_t price_scratch_bytes(size_t n);
 PriceScratch carve_price_scratch(void* base, size_t n);
+
+// Launch shape of a plain pricing launch: warps per block (each warp one
+// integral, so warps / 2 contracts per block) of the persistent grid, whether
+// the work queue takes contracts deepest-first (by |ln(K/S)| / sqrt(v0 T),
+// which ranks the bisection counts with a Spearman correlation of 0.9) or in
+// input order, and the share of the resident blocks per SM the grid fills.
+// Every shape gives bit-identical prices (a unit's arithmetic does not depend
+// on scheduling).
+struct LaunchShape {
+    int warps = 4;
+    int deepest_first = 0;
+    double occupancy = 1.0;
+};
+constexpr int kTuneClasses = 16;  // OPE_TUNE_CLASSES
+// Size classes of the tuning table: calls of at most kTuneClassMax[i]
+// contracts (64, 128, ..., 2^20; the last class: all larger calls).
+extern const uint64_t kTuneClassMax[kTuneClasses];
+// The shape a plain pricing launch of n contracts of `model` uses on the
+// current device: the tuned table's entry for n's class when this device has
+// been tuned and tuning is enabled, else the default shape.
+LaunchShape price_shape(int model, size_t n);
 
 // Device launchers (stream-ordered; all pointers are device pointers).
 // Contract c is priced with params + stride * p(c), where p(c) = param_idx[c]
@@ -128,10 +155,14 @@ struct PanelSink {
 size_t panel_sink_bytes(size_t n, int n_slots);  // panels + nbis for n contracts
 PanelSink carve_panel_sink(void* base, size_t n, int n_slots, const int32_t* slot);
 // sink (non-NULL): also store every priced integral's panel list there.
+// shape (non-NULL): this launch shape instead of price_shape(model, n); a
+// launch that stores panel lists (sink) or skips surfaces (surf_mask) always
+// uses 4 warps per block in input order.
 int launch_price_persistent(int model, const ope_contract* con, size_t n, const int64_t* surf_offsets,
                             size_t n_surf, const int32_t* param_idx, const double* params, double tol, double* out,
                             const PriceScratch& s, cudaStream_t st, int32_t* nbis_out = nullptr,
-                            const int32_t* surf_mask = nullptr, const PanelSink* sink = nullptr);
+                            const int32_t* surf_mask = nullptr, const PanelSink* sink = nullptr,
+                            const LaunchShape* shape = nullptr);
 // The adjoint's backward pass and combine (adjoint.cu) over panel lists a
 // pricing launch stored in `src`: out_grad (n x dim) = d price / d params.
 // bscratch: grad_backward_bytes(n, dim) bytes (chunk list, partial sums).

@@ -8,7 +8,12 @@
 // heston.rs:92-93 / bates.rs:58-59), integrated by one warp.  The two
 // integrals of a contract run on different warps; whichever finishes second
 // combines them into the price (heston.rs:95-98) through a per-contract
-// completion counter.
+// completion counter.  The queue takes contracts in input order, or
+// deepest-first (a counting sort of the contracts by a depth key, three small
+// kernels ahead of the launch) when the launch shape asks for it: the
+// reference's rayon pool (batch.rs:23-42) steals work per contract; here the
+// longest serial bisection chains start first, so a call's tail is not one
+// deep integral that started last.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -16,15 +21,13 @@
 #include "internal.h"
 #include "quadrature.cuh"
 
-// Launch shape of the pricing kernel: warps per block and, per model, the
-// minimum resident blocks per SM handed to __launch_bounds__ (which caps
-// registers per thread at 65536 / (32 * WARPS * MINB)): 64 registers x 8
-// blocks for both models, the fastest of 5-8 blocks on each model's full
-// batch (within 2 % of one another; kept per model because the optimum has
-// moved apart and back with changes to the node evaluation).
-#ifndef OPE_KERNEL_WARPS
-#define OPE_KERNEL_WARPS 4
-#endif
+// Register budget of the pricing kernel: per model, the minimum resident
+// blocks per SM of the 4-warp shape handed to __launch_bounds__ (registers
+// per thread capped at 65536 / (32 * 4 * MINB)); the 1- and 2-warp shapes get
+// 4 / warps times as many blocks, the same 64 registers.  8 for both models:
+// the fastest of 5-9 blocks on each model's full batch (within 2 % of one
+// another; kept per model because the optimum has moved apart and back with
+// changes to the node evaluation).
 #ifndef OPE_KERNEL_MINB_BATES
 #define OPE_KERNEL_MINB_BATES 8
 #endif
@@ -34,8 +37,16 @@
 
 namespace ope {
 
+namespace {
+constexpr int kOrderBuckets = 64;
+}
+
+// Layout: integ (2n doubles) | done (n) | head (256 B) | hist (2 x kOrderBuckets
+// counters, 512 B) | order (n) | bucket (n); done, head and hist are adjacent
+// so one memset clears them.
 size_t price_scratch_bytes(size_t n) {
-    return align_up(2 * n * sizeof(double), 256) + align_up(n * sizeof(unsigned int), 256) + 256;
+    return align_up(2 * n * sizeof(double), 256) + align_up(n * sizeof(unsigned int), 256) + 256 + 512 +
+           2 * align_up(n * sizeof(uint32_t), 256);
 }
 
 size_t panel_sink_bytes(size_t n, int n_slots) {
@@ -60,6 +71,12 @@ PriceScratch carve_price_scratch(void* base, size_t n) {
     s.done = reinterpret_cast<unsigned int*>(p);
     p += align_up(n * sizeof(unsigned int), 256);
     s.head = reinterpret_cast<unsigned long long*>(p);
+    p += 256;
+    s.hist = reinterpret_cast<unsigned int*>(p);
+    p += 512;
+    s.order = reinterpret_cast<uint32_t*>(p);
+    p += align_up(n * sizeof(uint32_t), 256);
+    s.bucket = reinterpret_cast<uint32_t*>(p);
     return s;
 }
 
@@ -70,15 +87,22 @@ struct ContractView {
     int opt_type;
 };
 
-__device__ __forceinline__ ContractView load_contract(const ope_contract* con, long long c) {
-    const ope_contract* p = con + c;
+// The 56-byte contract record staged cooperatively for the per-integral
+// constants: lanes 0-6 each load one of its seven 8-byte words (one coalesced
+// request), shuffles hand every lane the fields.  (The lane that combines a
+// contract's integrals at the end re-reads the fields it needs, so they are
+// not held across the integration.)
+__device__ __forceinline__ ContractView load_contract(const ope_contract* con, long long c, int lane) {
+    const unsigned FULL = 0xffffffffu;
+    const long long* w = reinterpret_cast<const long long*>(con + c);
+    const long long mine = lane < 7 ? __ldg(w + lane) : 0ll;
     ContractView v;
-    v.s = __ldg(&p->spot);
-    v.k = __ldg(&p->strike);
-    v.t = __ldg(&p->expiry);
-    v.r = __ldg(&p->rate);
-    v.q = __ldg(&p->div_yield);
-    v.opt_type = __ldg(&p->opt_type);
+    v.s = __longlong_as_double(__shfl_sync(FULL, mine, 0));
+    v.k = __longlong_as_double(__shfl_sync(FULL, mine, 1));
+    v.t = __longlong_as_double(__shfl_sync(FULL, mine, 2));
+    v.r = __longlong_as_double(__shfl_sync(FULL, mine, 3));
+    v.q = __longlong_as_double(__shfl_sync(FULL, mine, 4));
+    v.opt_type = (int)(unsigned)(__shfl_sync(FULL, mine, 6) & 0xffffffffll);  // low word of {opt_type, pad}
     return v;
 }
 
@@ -91,11 +115,11 @@ __device__ __forceinline__ void run_unit(long long c, int which, const ope_contr
                                          double tol, double* out, double* integ, unsigned int* done,
                                          int32_t* nbis_out, const PanelSink& sink, int slot, PanelStore& L,
                                          CfConsts& Cs, int lane, const LaneRule& R) {
-    const ContractView v = load_contract(con, c);
-    double pl[8];
-#pragma unroll
-    for (int i = 0; i < (BATES ? 8 : 5); ++i) pl[i] = __ldg(p + i);
     {
+        const ContractView v = load_contract(con, c, lane);
+        double pl[8];
+#pragma unroll
+        for (int i = 0; i < (BATES ? 8 : 5); ++i) pl[i] = __ldg(p + i);
         const CfConsts Cl = make_consts(v.s, v.k, v.t, v.r, pl, BATES, which);
         __syncwarp();
         if (lane == 0) Cs = Cl;
@@ -124,7 +148,9 @@ __device__ __forceinline__ void run_unit(long long c, int which, const ope_contr
             const double other = __ldcg(integ + 2 * c + (1 - which));
             const double i1 = which == 0 ? I : other;
             const double i2 = which == 0 ? other : I;
-            out[c] = finish_price(v.s, v.k, v.t, v.r, v.q, v.opt_type, i1, i2);
+            const ope_contract* k = con + c;
+            out[c] = finish_price(__ldg(&k->spot), __ldg(&k->strike), __ldg(&k->expiry), __ldg(&k->rate),
+                                  __ldg(&k->div_yield), __ldg(&k->opt_type), i1, i2);
         }
     }
 }
@@ -139,23 +165,29 @@ __device__ __forceinline__ long long find_surface(const int64_t* off, long long 
     return lo - 1;
 }
 
+__device__ __forceinline__ long long param_set(const int32_t* param_idx, const int64_t* surf_off, long long n_surf,
+                                               long long c) {
+    return param_idx ? (long long)__ldg(param_idx + c) : (n_surf > 1 ? find_surface(surf_off, n_surf, c) : 0);
+}
+
 // Every warp pulls units from the device queue until it drains; the grid is
-// the resident capacity of the GPU, or fewer warps than units for small calls.
-template <bool BATES, bool SAVE>
-__global__ void __launch_bounds__(OPE_KERNEL_WARPS * 32, BATES ? OPE_KERNEL_MINB_BATES : OPE_KERNEL_MINB_HESTON) k_price_persistent(const ope_contract* __restrict__ con, long long n,
-                                                          const int64_t* __restrict__ surf_off, long long n_surf,
-                                                          const int32_t* __restrict__ param_idx,
-                                                          const int32_t* __restrict__ surf_mask,
-                                                          const double* __restrict__ params, double tol,
-                                                          double* __restrict__ out, double* integ,
-                                                          unsigned int* done, unsigned long long* head,
-                                                          int32_t* nbis_out, PanelSink sink) {
+// the resident capacity of the GPU (or the launch shape's share of it), or
+// fewer warps than units for small calls.  Queue position q holds contract
+// order[q] (input order when order is NULL); its two integrals are units 2q
+// and 2q + 1, so a contract's pair starts together.
+template <bool BATES, bool SAVE, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, (BATES ? OPE_KERNEL_MINB_BATES : OPE_KERNEL_MINB_HESTON) * 4 / WARPS)
+    k_price_persistent(const ope_contract* __restrict__ con, long long n, const int64_t* __restrict__ surf_off,
+                       long long n_surf, const int32_t* __restrict__ param_idx, const int32_t* __restrict__ surf_mask,
+                       const double* __restrict__ params, double tol, double* __restrict__ out, double* integ,
+                       unsigned int* done, unsigned long long* head, int32_t* nbis_out, PanelSink sink,
+                       const uint32_t* __restrict__ order) {
     extern __shared__ PanelStore smem_panels[];
     // Per warp: the unit's integrand constants.  They are warp-uniform, so the
     // node evaluation reads them from shared memory (broadcast loads) and
     // leaves its registers to the per-lane values: at the 72-register cap
     // that cut the spills by half and the Bates batch's time by 4 %.
-    __shared__ CfConsts s_consts[OPE_KERNEL_WARPS];
+    __shared__ CfConsts s_consts[WARPS];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const LaneRule R = lane_rule(lane);
     const int stride = BATES ? 8 : 5;
@@ -165,13 +197,13 @@ __global__ void __launch_bounds__(OPE_KERNEL_WARPS * 32, BATES ? OPE_KERNEL_MINB
         if (lane == 0) unit = atomicAdd(head, 1ull);
         unit = __shfl_sync(0xffffffffu, unit, 0);
         if (unit >= n_units) break;
-        const long long c = (long long)(unit >> 1);
-        const long long s = param_idx ? (long long)__ldg(param_idx + c)
-                                      : (n_surf > 1 ? find_surface(surf_off, n_surf, c) : 0);
+        const long long q = (long long)(unit >> 1);
+        const long long c = order ? (long long)__ldg(order + q) : q;
+        const long long s = param_set(param_idx, surf_off, n_surf, c);
         if (surf_mask && __ldg(surf_mask + s) == 0) {
-            // a skipped surface's units are contiguous: move the queue head past
-            // all of them with one atomic instead of one per unit
-            if (lane == 0 && !param_idx && surf_off)
+            // a skipped surface's units are contiguous in input order: move the
+            // queue head past all of them with one atomic instead of one per unit
+            if (lane == 0 && !param_idx && surf_off && !order)
                 atomicMax(head, 2ull * (unsigned long long)__ldg(surf_off + s + 1));
             continue;
         }
@@ -183,64 +215,188 @@ __global__ void __launch_bounds__(OPE_KERNEL_WARPS * 32, BATES ? OPE_KERNEL_MINB
     }
 }
 
+// Depth bucket of a contract: 0 for the deepest.  The key |ln(K/S)| /
+// sqrt(v0 T) -- how many standard deviations of the initial variance over the
+// expiry the strike lies out -- ranks the integrals' bisection counts with a
+// Spearman correlation of 0.9 on the benchmark batches (short expiries and
+// deep wings need the most panels); 8 buckets per doubling of 1 + key.
+__device__ __forceinline__ unsigned depth_bucket(const ope_contract* con, long long c, double v0) {
+    const double x = fabs(log(__ldg(&con[c].strike) / __ldg(&con[c].spot)));
+    const double key = x / sqrt(fmax(v0, 0.0) * __ldg(&con[c].expiry));
+    if (!(key == key)) return kOrderBuckets - 1;  // NaN (e.g. 0/0): last
+    const int b = (int)fmin(8.0 * log2(1.0 + key), (double)(kOrderBuckets - 1));
+    return (unsigned)(kOrderBuckets - 1 - b);
+}
+
+__global__ void __launch_bounds__(256) k_order_bucket(const ope_contract* __restrict__ con, long long n,
+                                                      const int64_t* __restrict__ surf_off, long long n_surf,
+                                                      const int32_t* __restrict__ param_idx,
+                                                      const double* __restrict__ params, int stride,
+                                                      uint32_t* __restrict__ bucket, unsigned int* hist) {
+    __shared__ unsigned int h[kOrderBuckets];
+    for (int i = threadIdx.x; i < kOrderBuckets; i += blockDim.x) h[i] = 0;
+    __syncthreads();
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        const long long s = param_set(param_idx, surf_off, n_surf, c);
+        const unsigned b = depth_bucket(con, c, __ldg(params + s * stride));
+        bucket[c] = b;
+        atomicAdd(&h[b], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kOrderBuckets; i += blockDim.x)
+        if (h[i]) atomicAdd(hist + i, h[i]);
+}
+
+// Queue positions: each block forms the buckets' starting positions (an
+// exclusive prefix sum of the kOrderBuckets counts hist[0..64), one warp),
+// then each contract takes the next free slot of its bucket through the fill
+// counters hist[64..128) (the order inside a bucket is arbitrary, and
+// irrelevant to the prices).
+__global__ void __launch_bounds__(256) k_order_scatter(long long n, const uint32_t* __restrict__ bucket,
+                                                       unsigned int* hist, uint32_t* __restrict__ order) {
+    __shared__ unsigned int start[kOrderBuckets];
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        const unsigned a = __ldcg(hist + 2 * lane), b = __ldcg(hist + 2 * lane + 1);
+        unsigned incl = a + b;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const unsigned v = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) incl += v;
+        }
+        start[2 * lane] = incl - (a + b);
+        start[2 * lane + 1] = incl - b;
+    }
+    __syncthreads();
+    unsigned int* fill = hist + kOrderBuckets;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        const uint32_t b = bucket[c];
+        order[start[b] + atomicAdd(fill + b, 1u)] = (uint32_t)c;
+    }
+}
+
 template <class K>
-int persistent_grid(K kernel, int threads, size_t smem, int* grid) {
+int persistent_grid(K kernel, int threads, size_t smem, double occupancy, int* grid) {
     int per_sm = 0, sms = 0;
     OPE_TRY(blocks_per_sm(reinterpret_cast<const void*>(kernel), threads, smem, &per_sm));
     OPE_TRY(current_device_sms(&sms));
-    *grid = std::max(1, (int)(per_sm * sms * tctx().grid_fraction));
+    const int blocks = std::max(1, (int)(per_sm * occupancy));
+    *grid = std::max(1, (int)(blocks * sms * tctx().grid_fraction));
     return OPE_OK;
 }
 
-template <bool BATES, bool SAVE>
+template <bool BATES, bool SAVE, int WARPS>
 int launch_impl(const ope_contract* con, size_t n, const int64_t* surf_offsets, size_t n_surf,
                 const int32_t* param_idx, const double* params, double tol, double* out, const PriceScratch& s,
-                cudaStream_t st, int32_t* nbis_out, const int32_t* surf_mask, const PanelSink& sink) {
-    const int warps = OPE_KERNEL_WARPS, threads = warps * 32;
-    const size_t smem = warps * sizeof(PanelStore);
+                cudaStream_t st, int32_t* nbis_out, const int32_t* surf_mask, const PanelSink& sink,
+                const uint32_t* order, double occupancy) {
+    const int threads = WARPS * 32;
+    const size_t smem = WARPS * sizeof(PanelStore);
     int grid = 0;
-    OPE_TRY(persistent_grid(k_price_persistent<BATES, SAVE>, threads, smem, &grid));
-    const unsigned long long need = (2ull * n + warps - 1) / warps;
+    OPE_TRY(persistent_grid(k_price_persistent<BATES, SAVE, WARPS>, threads, smem, occupancy, &grid));
+    const unsigned long long need = (2ull * n + WARPS - 1) / WARPS;
     grid = (int)std::min<unsigned long long>((unsigned long long)grid, need);
-    k_price_persistent<BATES, SAVE><<<grid, threads, smem, st>>>(con, (long long)n, surf_offsets, (long long)n_surf,
-                                                                 param_idx, surf_mask, params, tol, out, s.integ,
-                                                                 s.done, s.head, nbis_out, sink);
+    k_price_persistent<BATES, SAVE, WARPS><<<grid, threads, smem, st>>>(
+        con, (long long)n, surf_offsets, (long long)n_surf, param_idx, surf_mask, params, tol, out, s.integ, s.done,
+        s.head, nbis_out, sink, order);
     OPE_CHECK(cudaGetLastError());
+    return OPE_OK;
+}
+
+template <bool BATES>
+int launch_plain(int warps, const ope_contract* con, size_t n, const int64_t* surf_offsets, size_t n_surf,
+                 const int32_t* param_idx, const double* params, double tol, double* out, const PriceScratch& s,
+                 cudaStream_t st, int32_t* nbis_out, const uint32_t* order, double occupancy) {
+    const PanelSink none{nullptr, nullptr, nullptr, 1};
+    switch (warps) {
+        case 1:
+            return launch_impl<BATES, false, 1>(con, n, surf_offsets, n_surf, param_idx, params, tol, out, s, st,
+                                                nbis_out, nullptr, none, order, occupancy);
+        case 2:
+            return launch_impl<BATES, false, 2>(con, n, surf_offsets, n_surf, param_idx, params, tol, out, s, st,
+                                                nbis_out, nullptr, none, order, occupancy);
+        default:
+            return launch_impl<BATES, false, 4>(con, n, surf_offsets, n_surf, param_idx, params, tol, out, s, st,
+                                                nbis_out, nullptr, none, order, occupancy);
+    }
+}
+
+// Deepest-first queue order of the n contracts into s.order (s.hist, zeroed
+// by the caller, and s.bucket as scratch).
+int build_order(int model, const ope_contract* con, size_t n, const int64_t* surf_offsets, size_t n_surf,
+                const int32_t* param_idx, const double* params, const PriceScratch& s, cudaStream_t st) {
+    int sms = 0;
+    OPE_TRY(current_device_sms(&sms));
+    const long long want = (long long)((n + 255) / 256);
+    const unsigned blocks = (unsigned)std::max(1ll, std::min<long long>(want, 8ll * sms));
+    k_order_bucket<<<blocks, 256, 0, st>>>(con, (long long)n, surf_offsets, (long long)n_surf, param_idx, params,
+                                           param_stride(model), s.bucket, s.hist);
+    OPE_CHECK(cudaGetLastError());
+    k_order_scatter<<<blocks, 256, 0, st>>>((long long)n, s.bucket, s.hist, s.order);
+    OPE_CHECK(cudaGetLastError());
+    tctx().launches += 2;
     return OPE_OK;
 }
 
 }  // namespace
 
+const uint64_t kTuneClassMax[kTuneClasses] = {1ull << 6,  1ull << 7,  1ull << 8,  1ull << 9,  1ull << 10, 1ull << 11,
+                                               1ull << 12, 1ull << 13, 1ull << 14, 1ull << 15, 1ull << 16, 1ull << 17,
+                                               1ull << 18, 1ull << 19, 1ull << 20, ~0ull};
+
 int prepare_price_kernels() {
-    const int threads = OPE_KERNEL_WARPS * 32;
-    const size_t smem = OPE_KERNEL_WARPS * sizeof(PanelStore);
     int grid = 0;
-    OPE_TRY(persistent_grid(k_price_persistent<false, false>, threads, smem, &grid));
-    OPE_TRY(persistent_grid(k_price_persistent<true, false>, threads, smem, &grid));
+    const int threads = 4 * 32;
+    const size_t smem = 4 * sizeof(PanelStore);
+    OPE_TRY(persistent_grid(k_price_persistent<false, false, 4>, threads, smem, 1.0, &grid));
+    OPE_TRY(persistent_grid(k_price_persistent<true, false, 4>, threads, smem, 1.0, &grid));
     return OPE_OK;
 }
 
 int launch_price_persistent(int model, const ope_contract* con, size_t n, const int64_t* surf_offsets,
                             size_t n_surf, const int32_t* param_idx, const double* params, double tol, double* out,
                             const PriceScratch& s, cudaStream_t st, int32_t* nbis_out, const int32_t* surf_mask,
-                            const PanelSink* sink) {
+                            const PanelSink* sink, const LaunchShape* shape) {
     if (n == 0) return OPE_OK;
-    // completion counters and queue head start at zero (one memset when adjacent)
+    const bool bates = model == OPE_MODEL_BATES;
+    // stored panel lists and skipped surfaces keep the fixed shape (4 warps,
+    // input order); the allocation-free entry point has no order scratch
+    LaunchShape sh;
+    if (!sink && !surf_mask) sh = shape ? *shape : price_shape(model, n);
+    if (!s.order || n > 0xffffffffull) sh.deepest_first = 0;
+    if (sh.warps != 1 && sh.warps != 2) sh.warps = 4;
+    if (!(sh.occupancy > 0.0 && sh.occupancy <= 1.0)) sh.occupancy = 1.0;
+    // completion counters, queue head and (for a deepest-first order) the
+    // bucket counters start at zero: one memset where they are adjacent
     const size_t done_bytes = align_up(n * sizeof(unsigned int), 256);
-    if (reinterpret_cast<char*>(s.head) == reinterpret_cast<char*>(s.done) + done_bytes) {
-        OPE_CHECK(cudaMemsetAsync(s.done, 0, done_bytes + sizeof(unsigned long long), st));
+    const bool adjacent = reinterpret_cast<char*>(s.head) == reinterpret_cast<char*>(s.done) + done_bytes;
+    const bool hist_adjacent = sh.deepest_first && reinterpret_cast<char*>(s.hist) == reinterpret_cast<char*>(s.head) + 256;
+    if (adjacent) {
+        OPE_CHECK(cudaMemsetAsync(s.done, 0, done_bytes + (hist_adjacent ? 256 + 512 : sizeof(unsigned long long)), st));
     } else {
         OPE_CHECK(cudaMemsetAsync(s.done, 0, n * sizeof(unsigned int), st));
         OPE_CHECK(cudaMemsetAsync(s.head, 0, sizeof(unsigned long long), st));
     }
-    const bool bates = model == OPE_MODEL_BATES;
+    if (sh.deepest_first && !(adjacent && hist_adjacent))
+        OPE_CHECK(cudaMemsetAsync(s.hist, 0, 2 * kOrderBuckets * sizeof(unsigned int), st));
+    const uint32_t* order = nullptr;
+    if (sh.deepest_first) {
+        OPE_TRY(build_order(model, con, n, surf_offsets, n_surf, param_idx, params, s, st));
+        order = s.order;
+    }
     if (sink) {
-        OPE_TRY((bates ? launch_impl<true, true> : launch_impl<false, true>)(
-            con, n, surf_offsets, n_surf, param_idx, params, tol, out, s, st, nbis_out, surf_mask, *sink));
-    } else {
+        OPE_TRY((bates ? launch_impl<true, true, 4> : launch_impl<false, true, 4>)(
+            con, n, surf_offsets, n_surf, param_idx, params, tol, out, s, st, nbis_out, surf_mask, *sink, nullptr,
+            1.0));
+    } else if (surf_mask) {
         const PanelSink none{nullptr, nullptr, nullptr, 1};
-        OPE_TRY((bates ? launch_impl<true, false> : launch_impl<false, false>)(
-            con, n, surf_offsets, n_surf, param_idx, params, tol, out, s, st, nbis_out, surf_mask, none));
+        OPE_TRY((bates ? launch_impl<true, false, 4> : launch_impl<false, false, 4>)(
+            con, n, surf_offsets, n_surf, param_idx, params, tol, out, s, st, nbis_out, surf_mask, none, nullptr,
+            1.0));
+    } else {
+        OPE_TRY((bates ? launch_plain<true> : launch_plain<false>)(sh.warps, con, n, surf_offsets, n_surf, param_idx,
+                                                                   params, tol, out, s, st, nbis_out, order,
+                                                                   sh.occupancy));
     }
     tctx().launches += 1;
     return OPE_OK;

@@ -103,6 +103,22 @@ _sig("ope_price_surfaces_noalloc", ctypes.c_int, [_i32, _vp, _sz, _vp, _sz, _vp,
 _sig("ope_measure_fp64_peak", ctypes.c_int, [ctypes.POINTER(_d), ctypes.POINTER(_d)])
 _sig("ope_trace_integral", ctypes.c_int, [_i32, _vp, _vp, _i32, _d, _vp, _i32, ctypes.POINTER(_i32), ctypes.POINTER(_d)])
 
+class LaunchShape(ctypes.Structure):
+    _fields_ = [("warps_per_block", ctypes.c_int32), ("deepest_first", ctypes.c_int32), ("occupancy", ctypes.c_double)]
+
+
+class TuneEntry(ctypes.Structure):
+    _fields_ = [("max_contracts", ctypes.c_uint64), ("shape", LaunchShape), ("ms_default", ctypes.c_double),
+                ("ms_tuned", ctypes.c_double)]
+
+
+TUNE_CLASSES = 16  # OPE_TUNE_CLASSES
+TUNE_QUICK = 1    # OPE_TUNE_QUICK
+_sig("ope_autotune", ctypes.c_int, [_i32, ctypes.c_uint32, ctypes.POINTER(TuneEntry)])
+_sig("ope_set_autotune", ctypes.c_int, [_i32])
+_sig("ope_get_tune_table", ctypes.c_int, [_i32, ctypes.POINTER(TuneEntry), ctypes.POINTER(_i32)])
+_sig("ope_set_tune_table", ctypes.c_int, [_i32, ctypes.POINTER(TuneEntry)])
+
 _lib = None
 
 

@@ -490,6 +490,49 @@ def measure_fp64_peak() -> tuple[float, float]:
     return f.value, ms.value
 
 
+def _tune_rows(entries) -> list[dict]:
+    return [{"max_contracts": int(e.max_contracts) if e.max_contracts < 2 ** 63 else None,
+             "warps_per_block": int(e.shape.warps_per_block), "deepest_first": bool(e.shape.deepest_first),
+             "occupancy": float(e.shape.occupancy), "ms_default": float(e.ms_default), "ms_tuned": float(e.ms_tuned)}
+            for e in entries]
+
+
+def autotune(model: int, quick: bool = False) -> list[dict]:
+    """Measure the pricing kernel's launch shapes on this device (ope_autotune)
+    and install the per-size-class table; returns its rows (the last class,
+    max_contracts None, is every larger call)."""
+    entries = (_lib.TuneEntry * _lib.TUNE_CLASSES)()
+    check(load().ope_autotune(model, _lib.TUNE_QUICK if quick else 0, entries))
+    return _tune_rows(entries)
+
+
+def set_autotune(enabled: bool) -> None:
+    """Use the tuned tables (True) or the default launch shape (False)."""
+    check(load().ope_set_autotune(1 if enabled else 0))
+
+
+def set_tune_table(model: int, rows: list[dict]) -> None:
+    """Install a table (rows as autotune / tune_table return them) on this device."""
+    if len(rows) != _lib.TUNE_CLASSES:
+        raise ValueError(f"expected {_lib.TUNE_CLASSES} rows")
+    entries = (_lib.TuneEntry * _lib.TUNE_CLASSES)()
+    for e, r in zip(entries, rows):
+        e.shape.warps_per_block = int(r["warps_per_block"])
+        e.shape.deepest_first = int(bool(r["deepest_first"]))
+        e.shape.occupancy = float(r["occupancy"])
+        e.ms_default = float(r.get("ms_default", 0.0))
+        e.ms_tuned = float(r.get("ms_tuned", 0.0))
+    check(load().ope_set_tune_table(model, entries))
+
+
+def tune_table(model: int) -> tuple[list[dict], bool]:
+    """The current device's table for `model`, and whether it was tuned."""
+    entries = (_lib.TuneEntry * _lib.TUNE_CLASSES)()
+    tuned = ctypes.c_int32()
+    check(load().ope_get_tune_table(model, entries, ctypes.byref(tuned)))
+    return _tune_rows(entries), bool(tuned.value)
+
+
 TRACE_FIELDS = 39  # OPE_TRACE_FIELDS
 MAX_STEPS = 200    # OPE_MAX_PANELS: the first panel + at most 199 bisections
 
@@ -581,4 +624,5 @@ __all__ = [
     "calibrate_global", "calibrate_heston_regularized", "calibrate_bates_regularized", "calibrate_heston_multistart",
     "calibrate_bates_multistart", "calibrate_heston_global", "calibrate_bates_global",
     "calibrate_heston_global_regularized", "calibrate_bates_global_regularized", "trace_integral",
+    "autotune", "set_autotune", "tune_table", "set_tune_table",
 ]

@@ -96,6 +96,49 @@ def test_oracle_corner_fixture_unchanged(oracle):
         assert list(nb) == e["oracle_bisections"]
 
 
+def _ref_inputs():
+    from ope_b200 import workloads as W
+
+    rows = []
+    with open(os.path.join(GOLD, "ref_inputs.txt")) as f:
+        for line in f:
+            if not line.strip() or line.startswith("#"):
+                continue
+            lhs, rhs = line.split(";")
+            model, *p = lhs.split()
+            c = rhs.split()
+            con = np.zeros(1, W.CONTRACT_DTYPE)
+            for k, v in zip(("spot", "strike", "expiry", "rate", "div_yield"), c[:5]):
+                con[k] = float(v)
+            con["opt_type"] = 1 if c[5] == "put" else 0
+            rows.append((model == "bates", np.array([[float(x) for x in p]]), con))
+    return rows
+
+
+def test_reference_pin_inputs_price_on_the_oracle(oracle):
+    """The contracts of ref_inputs.txt (the pin against the reference crate's
+    own outputs, oracle/ref_golden/) parse and price on the oracle."""
+    rows = _ref_inputs()
+    assert len(rows) == 120 + 256 + 12
+    for bates, p, c in rows[::37]:
+        assert np.isfinite(oracle.batch_price(c, p, bates, oracle.REF_TOL)[0])
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(GOLD, "ref_prices.txt")),
+                    reason="no reference outputs: tests/golden/ref_prices.txt is written by "
+                           "oracle/ref_golden/make_ref_golden.sh where cargo exists")
+def test_oracle_equals_the_reference_crate(oracle):
+    """Pinned by the reference itself: the oracle's prices at the reference's
+    tolerance equal the reference crate's (heston_price / bates_price) bit for
+    bit on every contract of ref_inputs.txt."""
+    with open(os.path.join(GOLD, "ref_prices.txt")) as f:
+        ref = [float(x) for x in f.read().split()]
+    rows = _ref_inputs()
+    assert len(ref) == len(rows)
+    for (bates, p, c), r in zip(rows, ref):
+        assert oracle.batch_price(c, p, bates, oracle.REF_TOL)[0] == r
+
+
 def test_oracle_trace_replays_its_own_quadrature(oracle):
     """The oracle's step trace of adaptive_gk (heston.rs:193-212) is the
     quadrature it runs: its last total is the integral, its step count is one
