@@ -381,23 +381,25 @@ def bench_greeks(args, w, dev, flush, stream) -> dict:
     d_out = torch.empty(n * 8, dtype=torch.float64, device=dev)
     lib = ope._lib.load()
 
-    def run(fn):
-        o = ope._lib.Options(tol=w.tol, flags=ope._lib.FLAG_DEVICE_PTRS, reserved=0, stream=stream.cuda_stream)
+    def run(fn, flags=0):
+        o = ope._lib.Options(tol=w.tol, flags=ope._lib.FLAG_DEVICE_PTRS | flags, reserved=0,
+                             stream=stream.cuda_stream)
         ope._lib.check(fn(ope.MODEL_BATES, d_con.data_ptr(), n, d_par.data_ptr(), d_out.data_ptr(),
                           ctypes.byref(o)))
 
     out = {"workload": f"c3-bates-deepwing first {n} contracts, surface 0's parameters", "n_contracts": n}
-    for name, fn in (("bump", lib.ope_batch_greeks_ex), ("ad", lib.ope_batch_greeks_ad)):
+    for name, fn, flags in (("bump", lib.ope_batch_greeks_ex, 0), ("ad", lib.ope_batch_greeks_ad, 0),
+                            ("analytic", lib.ope_batch_greeks_ad, ope._lib.FLAG_ANALYTIC_GREEKS)):
         for _ in range(max(args.warmup, 3)):
             flush.zero_()
-            run(fn)
+            run(fn, flags)
         torch.cuda.synchronize()
         ms = []
         for _ in range(args.steps):
             flush.zero_()
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(stream)
-            run(fn)
+            run(fn, flags)
             b.record(stream)
             torch.cuda.synchronize()
             ms.append(a.elapsed_time(b))
@@ -422,6 +424,12 @@ def bench_greeks(args, w, dev, flush, stream) -> dict:
         out["ad"]["cpu_baseline"] = {"value": 64 / dt, "unit": out["ad"]["unit"], "cores": 1, "kind": "port",
                                      "sample": f"64 contracts, one thread, {dt:.1f} s"}
         out["ad"]["max_abs_vega_rel_err"] = float(np.max(np.abs(ad["vega"] - refad[:, 3]) / np.abs(refad[:, 3])))
+        an = ope.batch_greeks_ad(ope.MODEL_BATES, con[pick[:64]], par, tol=w.tol, analytic=True)
+        out["analytic"]["max_abs_vega_rel_err"] = float(np.max(np.abs(an["vega"] - refad[:, 3])
+                                                               / np.abs(refad[:, 3])))
+        out["analytic"]["cpu_baseline"] = out["ad"]["cpu_baseline"]
+    out["analytic"]["what"] = ("all eight Greeks as exact derivatives: one pricing + one backward pass of seven "
+                               "derivative integrals (OPE_FLAG_ANALYTIC_GREEKS)")
     return out
 
 

@@ -54,6 +54,7 @@ enum { OPE_MODEL_HESTON = 0, OPE_MODEL_BATES = 1 };
 #define OPE_REF_TOL 1e-8          /* heston.rs:228 */
 #define OPE_MAX_PANELS 200        /* heston.rs:194 */
 #define OPE_FLAG_DEVICE_PTRS 1u
+#define OPE_FLAG_ANALYTIC_GREEKS 2u  /* ope_batch_greeks_ad: all eight Greeks by adjoint, no bumps */
 
 /* ------------------------------------------------------------- records */
 /* types.rs:16-25 OptionContract (`vol` is carried but unused by Heston/Bates,
@@ -106,7 +107,7 @@ typedef struct {
 
 typedef struct {
     double tol;        /* absolute GK15 tolerance; <= 0 selects OPE_REF_TOL */
-    uint32_t flags;    /* OPE_FLAG_DEVICE_PTRS */
+    uint32_t flags;    /* OPE_FLAG_DEVICE_PTRS, OPE_FLAG_ANALYTIC_GREEKS */
     uint32_t reserved;
     void* stream;      /* cudaStream_t; used with OPE_FLAG_DEVICE_PTRS; NULL = default stream */
 } ope_options;
@@ -188,6 +189,15 @@ int ope_price_surfaces(int32_t model, const ope_contract* contracts, size_t n,
  * volga from the same derivative at v0 = (sqrt(v0) +- 0.01)^2 (lower leg
  * floored at 1e-6), delta / gamma (spot +- 1%), theta (T - 1 day, floored at
  * 1e-6), rho (r +- 1bp) and vanna by the reference's finite differences.
+ * With OPE_FLAG_ANALYTIC_GREEKS: every Greek is an exact derivative instead
+ * (the analytic S/r/T sensitivities that ad.rs:751-763 leaves to finite
+ * differences): one pricing and one backward pass of seven derivative
+ * integrals over the pricing's own panels -- in x = ln(S/K) (first and
+ * second order), r, T and v0 (first and second order, and mixed with x) --
+ * combined with the discount and parity terms of heston.rs:70, 95-98, in the
+ * same conventions: delta = dP/dS, gamma = d2P/dS2, vega = dP/dsqrt(v0),
+ * theta = -dP/dT per year, rho = dP/dr, vanna = d2P/dS dsqrt(v0),
+ * volga = d2P/dsqrt(v0)^2.
  * Host or device pointers (OPE_FLAG_DEVICE_PTRS). */
 int ope_batch_greeks_ad(int32_t model, const ope_contract* contracts, size_t n, const void* params,
                         ope_pricing_result* out, const ope_options* opts);

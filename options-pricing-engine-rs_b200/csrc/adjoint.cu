@@ -259,6 +259,145 @@ __global__ void k_grad_combine(const ope_contract* __restrict__ con, long long n
     for (int k = 0; k < DIM; ++k) out_grad[c * DIM + k] = seq * (d[0][k] / PI) - ker * (d[1][k] / PI);
 }
 
+// The analytic Greeks' backward pass: the work list of k_grad_backward
+// (chunks of stored panels), per node the seven Greek integrands of
+// cf_adjoint.cuh (d/dx, d2/dx2, d/dr, d/dT, d/dv0, d2/dx dv0, d2/dv0^2 of the
+// node value), a warp sum per chunk.  One parameter set per contract, as the
+// reference's AD Greeks take (ad.rs:736-865).
+template <bool BATES>
+__global__ void __launch_bounds__(128, OPE_GRAD_MINB) k_greeks_backward(const ope_contract* __restrict__ con, long long n,
+                                                        const int64_t* __restrict__ surf_off, long long n_surf,
+                                                        const int32_t* __restrict__ param_idx,
+                                                        const double* __restrict__ params, PanelSink src,
+                                                        BackScratch B) {
+    constexpr int DIM = BATES ? 8 : 5;
+    const int lane = threadIdx.x & 31;
+    const LaneRule R = lane_rule(lane);
+    const unsigned long long n_work = *(volatile unsigned long long*)B.count;  // final: set by k_grad_chunks
+    while (true) {
+        unsigned long long w = 0;
+        if (lane == 0) w = atomicAdd(B.count + 1, 1ull);
+        w = __shfl_sync(0xffffffffu, w, 0);
+        if (w >= n_work) break;
+        const unsigned long long e = __ldg(B.work + w);
+        const unsigned long long unit = e >> 3;
+        const int chunk = (int)(e & 7ull);
+        if (!ope_check(unit < 2ull * (unsigned long long)n && chunk < kMaxChunks, CHK_PANEL_INDEX)) continue;
+        const long long c = (long long)(unit >> 1);
+        const int which = (int)(unit & 1);
+        const long long s = unit_surface(param_idx, surf_off, n_surf, c);
+        const double* p = params + s * DIM;
+        double pl[8];
+#pragma unroll
+        for (int i = 0; i < DIM; ++i) pl[i] = __ldg(p + i);
+        const ope_contract* cp = con + c;
+        const double r = __ldg(&cp->rate);
+        const CfConsts C = make_consts(__ldg(&cp->spot), __ldg(&cp->strike), __ldg(&cp->expiry), r, pl, BATES, which);
+        const double is2 = 1.0 / (pl[3] * pl[3]);
+        const double lambda = BATES ? pl[5] : 0.0;
+        int slot = src.slot ? __ldg(src.slot + s) : 0;
+        if (!ope_check(slot >= 0 && slot < src.n_slots, CHK_SLOT)) slot = 0;
+        const size_t pidx = (size_t)unit * src.n_slots + slot;
+        int len = __ldg(src.nbis + pidx) + 1;
+        if (!ope_check(len >= 1 && len <= kMaxPanels, CHK_PANEL_LEN)) len = len < 1 ? 1 : kMaxPanels;
+        const int p0 = chunk * kChunkPanels, p1 = min(len, p0 + kChunkPanels);
+        const double* P = src.panels + pidx * (2 * kMaxPanels) + 2 * p0;
+        double acc[7];
+#pragma unroll
+        for (int k = 0; k < 7; ++k) acc[k] = 0.0;
+        const int items = 15 * max(p1 - p0, 0);
+        for (int base = 0; base < items; base += 32) {
+            const int idx = base + lane;
+            const int pi = idx / 15, j = idx - 15 * (idx / 15);
+            const double xj = __shfl_sync(0xffffffffu, R.x, j & 15);
+            const double wj = __shfl_sync(0xffffffffu, R.wk, j & 15);
+            if (idx < items) {
+                const double a = __ldg(P + 2 * pi), b = __ldg(P + 2 * pi + 1);
+                const double cc = 0.5 * (a + b), h = 0.5 * (b - a);
+                const double tn = __dadd_rn(cc, __dmul_rn(h, xj));
+                const double omt = 1.0 - tn;
+                const double itt = rcp_nr(omt * tn);  // 1 / ((1 - t) t)
+                const double u = node_u(omt, tn, itt);
+                C2 Zv, ZT;
+                const C2 Z = exponent_and_greeks<BATES>(C, u, r, lambda, is2, Zv, ZT);
+                greeks_accumulate(Z, Zv, ZT, u, C.t, (tn > 0.0) && (u >= 1e-12), itt, h * wj, acc);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 7; ++k) acc[k] = warp_sum(acc[k]);
+        if (lane == 0) {
+            double* out = B.part + w * 7;
+#pragma unroll
+            for (int k = 0; k < 7; ++k) out[k] = acc[k];
+        }
+    }
+}
+
+// Per contract: the eight Greeks from the two integrals (I1, I2 of the
+// pricing launch), their seven derivative integrals and the Gil-Pelaez
+// combination (heston.rs:95-98, 70), in the reference's conventions
+// (greeks.rs:19-72): delta = dP/dS, gamma = d2P/dS2, vega = dP/dsqrt(v0),
+// theta = -dP/dT (per year), rho = dP/dr, vanna = d2P/dS dsqrt(v0),
+// volga = d2P/dsqrt(v0)^2.  With a = S e^{-qT}, b = K e^{-rT},
+// P_j = 1/2 + I_j/pi and x = ln(S/K), the call a P1 - b P2 gives
+//   dC/dS  = e^{-qT} P1 + e^{-qT} I1x/pi - b I2x/(pi S)
+//   dC2/dS2 = e^{-qT} (I1x + I1xx)/(pi S) - b (I2xx - I2x)/(pi S^2)
+//   dC/dr  = a I1r/pi + T b P2 - b I2r/pi,  dC/dT = -q a P1 + a I1T/pi + r b P2 - b I2T/pi
+// and the v0 terms alike; where the reference clamps the call at 0 its
+// derivatives are 0; the put (C - a + b) adds -e^{-qT}, -T b and q a - r b.
+template <int DIM>
+__global__ void k_greeks_combine(const ope_contract* __restrict__ con, long long n, const double* __restrict__ integ,
+                                 const double* __restrict__ price, const double* __restrict__ params, BackScratch B,
+                                 ope_pricing_result* __restrict__ out) {
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    double G[2][7];
+#pragma unroll
+    for (int which = 0; which < 2; ++which) {
+        const long long u = 2 * c + which;
+        const double* part = B.part + (size_t)B.unit_base[u] * 7;
+        const int nc = B.nch[u];
+#pragma unroll
+        for (int k = 0; k < 7; ++k) G[which][k] = 0.0;
+        for (int j = 0; j < nc; ++j)
+#pragma unroll
+            for (int k = 0; k < 7; ++k) G[which][k] += part[j * 7 + k];
+    }
+    const ope_contract& k = con[c];
+    const double PI = 3.14159265358979323846;
+    const double S = k.spot, T = k.expiry, r = k.rate, q = k.div_yield, v0 = params[0];
+    const double eq = exp(-q * T), er = exp(-r * T);
+    const double a = S * eq, b = k.strike * er;
+    const double p1 = 0.5 + integ[2 * c] / PI, p2 = 0.5 + integ[2 * c + 1] / PI;
+    const bool live = a * p1 - b * p2 > 0.0;  // heston.rs:98: the call is clamped at 0
+    double dS = 0.0, dSS = 0.0, dr = 0.0, dT = 0.0, dv = 0.0, dSv = 0.0, dvv = 0.0;
+    if (live) {
+        dS = eq * p1 + eq * G[0][0] / PI - b * G[1][0] / (PI * S);
+        dSS = eq * (G[0][0] + G[0][1]) / (PI * S) - b * (G[1][1] - G[1][0]) / (PI * S * S);
+        dr = a * G[0][2] / PI + T * b * p2 - b * G[1][2] / PI;
+        dT = -q * a * p1 + a * G[0][3] / PI + r * b * p2 - b * G[1][3] / PI;
+        dv = (a * G[0][4] - b * G[1][4]) / PI;
+        dSv = eq * G[0][4] / PI + eq * G[0][5] / PI - b * G[1][5] / (PI * S);
+        dvv = (a * G[0][6] - b * G[1][6]) / PI;
+    }
+    if (k.opt_type != 0) {  // put = call - S e^{-qT} + K e^{-rT} (heston.rs:70)
+        dS -= eq;
+        dr -= T * b;
+        dT += q * a - r * b;
+    }
+    const double sv = sqrt(v0);
+    ope_pricing_result o;
+    o.price = price[c];
+    o.delta = dS;
+    o.gamma = dSS;
+    o.vega = 2.0 * sv * dv;
+    o.theta = -dT;
+    o.rho = dr;
+    o.vanna = 2.0 * sv * dSv;
+    o.volga = 2.0 * dv + 4.0 * v0 * dvv;
+    out[c] = o;
+}
+
 template <class K>
 int grad_grid(K kernel, size_t smem, unsigned long long need, int* grid) {
     int per_sm = 0;
@@ -335,6 +474,50 @@ int launch_grad_backward(int model, const ope_contract* con, size_t n, const int
     else
         k_grad_combine<5><<<cb, 128, 0, st>>>(con, (long long)n, surf_offsets, (long long)n_surf, param_idx, surf_mask,
                                               B, out_grad);
+    OPE_CHECK(cudaGetLastError());
+    tctx().launches += 3;
+    return OPE_OK;
+}
+
+size_t greeks_analytic_workspace_bytes(size_t n) {
+    return align_up(n * sizeof(double), 256) + price_scratch_bytes(n) + panel_sink_bytes(n, 1) +
+           grad_backward_bytes(n, 5);  // 5 + 2 = 7 sums per chunk
+}
+
+int launch_greeks_analytic(int model, const ope_contract* con, size_t n, const double* params, double tol,
+                           ope_pricing_result* out, void* ws, cudaStream_t st) {
+    if (n == 0) return OPE_OK;
+    char* p = static_cast<char*>(ws);
+    double* price = reinterpret_cast<double*>(p);
+    p += align_up(n * sizeof(double), 256);
+    const PriceScratch s = carve_price_scratch(p, n);
+    p += price_scratch_bytes(n);
+    const PanelSink sink = carve_panel_sink(p, n, 1, nullptr);
+    p += panel_sink_bytes(n, 1);
+    const BackScratch B = carve_back_scratch(p, n, 5);
+    // 1. prices, the integrals I1, I2 (s.integ) and the final panel lists
+    OPE_TRY(launch_price_persistent(model, con, n, nullptr, 1, nullptr, params, tol, price, s, st, nullptr, nullptr,
+                                    &sink));
+    // 2. the Greek integrals over those panels, 3. the combination
+    OPE_CHECK(cudaMemsetAsync(B.count, 0, 2 * sizeof(unsigned long long), st));
+    const unsigned long long units = 2ull * n;
+    k_grad_chunks<<<(unsigned)((units + 127) / 128), 128, 0, st>>>((long long)n, nullptr, 1, nullptr, nullptr, sink, B);
+    OPE_CHECK(cudaGetLastError());
+    const unsigned long long need = (units * kMaxChunks + 3) / 4;
+    int grid = 0;
+    if (model == OPE_MODEL_BATES) {
+        OPE_TRY(grad_grid(k_greeks_backward<true>, 0, need, &grid));
+        k_greeks_backward<true><<<grid, 128, 0, st>>>(con, (long long)n, nullptr, 1, nullptr, params, sink, B);
+    } else {
+        OPE_TRY(grad_grid(k_greeks_backward<false>, 0, need, &grid));
+        k_greeks_backward<false><<<grid, 128, 0, st>>>(con, (long long)n, nullptr, 1, nullptr, params, sink, B);
+    }
+    OPE_CHECK(cudaGetLastError());
+    const unsigned cb = (unsigned)((n + 127) / 128);
+    if (model == OPE_MODEL_BATES)
+        k_greeks_combine<8><<<cb, 128, 0, st>>>(con, (long long)n, s.integ, price, params, B, out);
+    else
+        k_greeks_combine<5><<<cb, 128, 0, st>>>(con, (long long)n, s.integ, price, params, B, out);
     OPE_CHECK(cudaGetLastError());
     tctx().launches += 3;
     return OPE_OK;

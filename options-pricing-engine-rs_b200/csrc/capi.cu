@@ -251,8 +251,11 @@ int batch_greeks(int32_t model, const ope_contract* contracts, size_t n, const v
     if (!contracts || !params || !out) return set_error(OPE_ERR_INVALID_ARG, "NULL array argument");
     OPE_TRY(ensure_device());
     const int stride = param_stride(model);
-    const size_t g_bytes = ad ? greeks_ad_workspace_bytes(n, stride) : greeks_workspace_bytes(n);
+    const bool analytic = ad && opts && (opts->flags & OPE_FLAG_ANALYTIC_GREEKS);
+    const size_t g_bytes = analytic ? greeks_analytic_workspace_bytes(n)
+                                    : (ad ? greeks_ad_workspace_bytes(n, stride) : greeks_workspace_bytes(n));
     auto launch = [&](const ope_contract* con, const double* par, ope_pricing_result* o, void* gws, cudaStream_t st) {
+        if (analytic) return launch_greeks_analytic(model, con, n, par, tol, o, gws, st);
         return ad ? launch_greeks_ad(model, con, n, par, tol, o, gws, st) : launch_greeks(model, con, n, par, tol, o, gws, st);
     };
     if (device_ptrs(opts)) {

@@ -172,4 +172,85 @@ __device__ __forceinline__ void node_accumulate(const C2& Z, const C2* dz, bool 
     }
 }
 
+// The exponent Z of one node with its derivatives with respect to v0 and
+// to the expiry T, for the analytic Greeks (x = ln(S/K) and r enter Z as
+// i u x and i u r T -- the P1 normaliser's r T cancels the real part of
+// i r phi T -- so their derivatives need nothing from here):
+//   dZ/dv0 = Dh / sigma^2
+//   dZ/dT  = kts (m - 2 g d e / (1 - g e)) + v0s m d e (1 - g) / (1 - g e)^2 + i r u [+ lambda base]
+// with m = xi - d, e = exp(-d T) (de/dT = -d e), and for Bates J = lambda T base
+// (the normaliser's own T-dependence, r T, is already taken out: the jump
+// factor at phi = -i is 1 and C, D vanish there).
+template <bool BATES>
+__device__ __forceinline__ C2 exponent_and_greeks(const CfConsts& C, double u, double r, double lambda, double is2,
+                                                  C2& Zv, C2& ZT) {
+    const double T = C.t;
+    const C2 xi = c2(C.kappa + C.rs * C.phi_im, -C.rs * u);
+    const C2 wphi = c2(u * u, C.sgn * u);  // phi(phi+i)
+    const C2 z = xi * xi + wphi * C.sig2;
+    C2 d;
+    csqrt_node(z.re, z.im, d.re, d.im);
+    const C2 m = xi - d, p = xi + d;
+    const C2 g = m * crcp(p);
+    double sn, cs;
+    sincos(-d.im * T, &sn, &cs);
+    const double em = exp(-d.re * T);
+    const C2 e = c2(em * cs, em * sn);
+    const C2 ge = g * e;
+    const C2 N = c2(ge.re - 1.0, ge.im);  // g e - 1
+    const C2 A = N * crcp(c2(g.re - 1.0, g.im));
+    const C2 lnA = c2(0.5 * log(A.re * A.re + A.im * A.im), atan2_node(A.im, A.re));
+    const C2 iN = crcp(N);
+    const C2 iQ = c2(-iN.re, -iN.im);  // 1/(1 - g e)
+    const C2 om = c2(1.0 - e.re, -e.im);
+    const C2 Ch = m * T - lnA * 2.0;
+    const C2 Dh = m * om * iQ;
+    C2 Z = Ch * C.kts + Dh * C.v0s + c2(-C.rt * C.phi_im + C.lnm_re, C.rt * u + u * C.x + C.lnm_im);
+    Zv = Dh * is2;
+    const C2 de = d * e;
+    const C2 dCh = m - g * de * iQ * 2.0;
+    const C2 dDh = m * de * c2(1.0 - g.re, -g.im) * (iQ * iQ);
+    ZT = dCh * C.kts + dDh * C.v0s + c2(0.0, r * u);
+    if (BATES) {
+        const C2 iphi = c2(-C.phi_im, u);
+        const C2 phi2 = c2(u * u - C.phi_im * C.phi_im, 2.0 * u * C.phi_im);
+        double js, jc;
+        sincos(u * C.mu_j - C.hs2 * phi2.im, &js, &jc);
+        const double je = exp(-C.phi_im * C.mu_j - C.hs2 * phi2.re);
+        const C2 base = c2(je * jc, je * js) - c2(1.0, 0.0) - iphi * C.comp;
+        Z = Z + base * C.lt;
+        ZT = ZT + base * lambda;
+    }
+    return Z;
+}
+
+// Sums of the analytic-Greek integrands of one node into acc[0..7):
+// d/dx, d2/dx2, d/dr, d/dT, d/dv0, d2/dx dv0, d2/dv0^2 of g = Im(W) / (u t^2),
+// weighted by hw; with Z linear in x (i u x) and in v0 (v0 Dh / sigma^2) the
+// second derivatives are Im(W Zp Zq) / (u t^2).  A node outside the
+// substitution's domain or with a non-finite value contributes zero.
+__device__ __forceinline__ void greeks_accumulate(const C2& Z, const C2& Zv, const C2& ZT, double u, double T,
+                                                  bool inside, double itt, double hw, double* acc) {
+    double sn, cs;
+    sincos(Z.im, &sn, &cs);
+    const double ez = exp(Z.re);
+    const C2 Wf = c2(ez * cs * itt, ez * sn * itt);
+    const C2 Wv = Wf * Zv;
+    double g[7];
+    g[0] = u * Wf.re;        // Im(W i u)
+    g[1] = -u * u * Wf.im;   // Im(W (i u)^2)
+    g[2] = u * T * Wf.re;    // Im(W i u T)
+    g[3] = (Wf * ZT).im;
+    g[4] = Wv.im;
+    g[5] = u * Wv.re;        // Im(W Zv i u)
+    g[6] = (Wv * Zv).im;
+    bool ok = inside && isfinite(Wf.im);
+#pragma unroll
+    for (int k = 0; k < 7; ++k) ok = ok && isfinite(g[k]);
+    if (ok) {
+#pragma unroll
+        for (int k = 0; k < 7; ++k) acc[k] += hw * g[k];
+    }
+}
+
 }  // namespace ope

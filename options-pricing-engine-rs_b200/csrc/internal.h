@@ -233,6 +233,14 @@ size_t greeks_ad_workspace_bytes(size_t n, int dim);
 int launch_greeks_ad(int model, const ope_contract* con, size_t n, const double* params, double tol,
                      ope_pricing_result* out, void* ws, cudaStream_t st);
 
+// All eight Greeks analytically (adjoint.cu): one pricing launch that keeps
+// the panel lists, one backward pass of the seven Greek integrals, one
+// combine; n contracts under one parameter set; `ws` must hold
+// greeks_analytic_workspace_bytes(n) bytes.
+size_t greeks_analytic_workspace_bytes(size_t n);
+int launch_greeks_analytic(int model, const ope_contract* con, size_t n, const double* params, double tol,
+                           ope_pricing_result* out, void* ws, cudaStream_t st);
+
 inline int param_stride(int model) { return model == OPE_MODEL_BATES ? 8 : 5; }
 
 }  // namespace ope

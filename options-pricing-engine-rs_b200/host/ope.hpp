@@ -194,6 +194,23 @@ inline PricingResult bates_greeks_ad(double spot, double strike, double expiry, 
     return r;
 }
 
+// All eight Greeks as exact derivatives (OPE_FLAG_ANALYTIC_GREEKS): the
+// analytic S / r / T sensitivities ad.rs:751-763 leaves to finite differences,
+// for many contracts under one parameter set (5 or 8 doubles by model).
+inline std::vector<PricingResult> batch_greeks_analytic(int32_t model, const std::vector<OptionContract>& contracts,
+                                                        const double* params, double tol = OPE_REF_TOL) {
+    std::vector<PricingResult> out(contracts.size());
+    if (contracts.empty()) return out;
+    std::vector<ope_contract> c;
+    c.reserve(contracts.size());
+    for (const auto& k : contracts)
+        c.push_back(ope_contract{k.spot, k.strike, k.expiry, k.rate, k.div_yield, k.vol,
+                                 static_cast<int32_t>(k.opt_type), 0});
+    ope_options o{tol, OPE_FLAG_ANALYTIC_GREEKS, 0, nullptr};
+    check(ope_batch_greeks_ad(model, c.data(), c.size(), params, out.data(), &o));
+    return out;
+}
+
 // ad.rs heston_greeks_ad5: the joint five-parameter pass returns what
 // heston_greeks_ad returns (ad.rs:1295-1322), so it is the same computation.
 inline PricingResult heston_greeks_ad5(double spot, double strike, double expiry, double rate, double div_yield,

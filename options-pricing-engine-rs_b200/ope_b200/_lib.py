@@ -25,6 +25,7 @@ STATUS_NAMES = {
     8: "OPE_ERR_NOT_FOUND",
 }
 FLAG_DEVICE_PTRS = 1
+FLAG_ANALYTIC_GREEKS = 2
 MODEL_HESTON, MODEL_BATES = 0, 1
 
 

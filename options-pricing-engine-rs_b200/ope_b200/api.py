@@ -172,16 +172,18 @@ def batch_bates_greeks(contracts, params, tol=REF_TOL) -> np.ndarray:
     return _batch_greeks(MODEL_BATES, contracts, params, tol)
 
 
-def batch_greeks_ad(model: int, contracts, params, tol=REF_TOL) -> np.ndarray:
+def batch_greeks_ad(model: int, contracts, params, tol=REF_TOL, analytic: bool = False) -> np.ndarray:
     """ad.rs:736-795 / 809-865 for many contracts under one parameter set: vega and
     volga from the exact d price / d v0 (adjoint kernel), the rest by the
-    reference's finite differences.  Structured array of PricingResult."""
+    reference's finite differences.  analytic=True: all eight Greeks as exact
+    derivatives (OPE_FLAG_ANALYTIC_GREEKS) from one pricing and one backward
+    pass.  Structured array of PricingResult."""
     con = contracts_array(contracts)
     p = _params_array(params, model)
     out = np.zeros(con.size, dtype=RESULT_DTYPE)
     if con.size == 0:
         return out
-    o = _opts(tol)
+    o = _opts(tol, _lib.FLAG_ANALYTIC_GREEKS if analytic else 0)
     check(load().ope_batch_greeks_ad(model, con.ctypes.data, con.size, p.ctypes.data, out.ctypes.data,
                                      ctypes.byref(o)))
     return out
