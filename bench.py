@@ -67,7 +67,8 @@ def parse_args():
     ap.add_argument("--no-gradient", action="store_true", help="skip the adjoint-gradient section")
     ap.add_argument("--grad-n", type=int, default=1 << 18, help="contracts in the adjoint-gradient section")
     ap.add_argument("--no-serving", action="store_true", help="skip the config-5 serving section")
-    ap.add_argument("--serving-rates", default="100,1000,5000,20000")
+    ap.add_argument("--serving-rates", default="100,1000,5000,10000,15000,20000")
+    ap.add_argument("--serving-seconds", type=float, default=10.0, help="seconds of arrivals per serving rate")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shape (no ope_autotune)")
     return ap.parse_args()
 
@@ -503,23 +504,40 @@ def bench_implied_vol(args, w, dev, flush, stream, d_con, d_prices, prices) -> d
     return out
 
 
-def bench_serving(args) -> dict:
+def bench_serving(args, tuned: bool) -> dict:
     """Config 5: Poisson arrivals, 80 % Bates surface reprices / 20 % Heston
-    calibrations, sizes log-uniform in [20, 2000] contracts, rates swept."""
+    calibrations, sizes log-uniform in [20, 2000] contracts.  For every offered
+    rate a fresh stream with --serving-seconds of arrivals (contents drawn from
+    a pool of 3,000 distinct requests), then up to 20 s to drain; latencies
+    over the steady half of the arrivals.  The highest offered rate whose
+    reprices all finish and whose reprice latency does not grow across the
+    run is reported as the sustained reprice rate.  With the autotuner on, the
+    5,000 req/s stream is run once more with the default launch shape."""
+    import ope_b200 as ope
     from ope_b200 import serving as SV
 
-    out = {"mix": "80% Bates reprice / 20% Heston calibration, sizes log-uniform [20, 2000]", "rates": []}
-    pool = SV.make_stream(1200, seed=5)
+    out = {"mix": "80% Bates reprice / 20% Heston calibration, sizes log-uniform [20, 2000]",
+           "seconds_of_arrivals_per_rate": args.serving_seconds, "rates": []}
+    pool = SV.make_stream(3000, seed=5)
     with SV.Server(hbm_fraction=0.25, max_inflight=4) as srv:
-        # warm: one request of each kind
-        for r in pool[:8]:
+        # warm: a few requests of each kind
+        for r in pool[:16]:
             rid = srv.submit_price(1, r.contracts, r.params) if r.kind == 0 else srv.submit_calibrate(
                 0, r.contracts, r.iv, r.params)
             srv.wait(rid)
+        sustained = None
         for rate in [float(x) for x in args.serving_rates.split(",")]:
-            n = int(min(len(pool), max(150, rate * 1.5)))
-            res = SV.run_stream(srv, pool[:n], rate, seed=int(rate))
-            out["rates"].append(SV.summarize(res))
+            res = SV.run_sustained(srv, pool, rate, args.serving_seconds, seed=int(rate))
+            row = SV.summarize_sustained(res)
+            out["rates"].append(row)
+            if row["reprice_sustained"]:
+                sustained = rate
+        out["highest_offered_rate_with_reprices_sustained"] = sustained
+        if tuned:
+            ope.set_autotune(False)
+            res = SV.run_sustained(srv, pool, 5000.0, min(5.0, args.serving_seconds), seed=5000)
+            ope.set_autotune(True)
+            out["default_launch_shape_at_5000_req_per_s"] = SV.summarize_sustained(res)
         st = srv.stats()
     out["server"] = {k: st[k] for k in ("batches", "batched_requests", "max_inflight", "rejected",
                                          "hbm_budget_bytes", "hbm_peak_bytes")}
@@ -768,7 +786,7 @@ def run_ours(args) -> None:
     if rank == 0 and world == 1 and not args.no_calib:
         line["calibration"] = bench_calibration(args)
     if rank == 0 and world == 1 and not args.no_serving:
-        line["serving"] = bench_serving(args)
+        line["serving"] = bench_serving(args, tune is not None)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -34,10 +34,14 @@
 #include "internal.h"
 #include "quadrature.cuh"
 
-// Minimum resident blocks per SM for the adjoint kernel's __launch_bounds__
-// (caps registers per thread at 65536 / (128 * OPE_GRAD_MINB)).
+// Minimum resident blocks per SM for the backward kernels' __launch_bounds__
+// (caps registers per thread at 65536 / (128 * OPE_GRAD_MINB)): 5, i.e. 96
+// registers.  The kernel time is flat from 4 to 7 blocks (within 0.5 % on the
+// 262k-contract Bates gradient, 1 % on the Heston one), but at 7 blocks (72
+// registers) its spills overflow L1: 274 MB of DRAM writes per 65,536 Bates
+// contracts against 12 MB at 5 blocks (ncu, one launch).
 #ifndef OPE_GRAD_MINB
-#define OPE_GRAD_MINB 7
+#define OPE_GRAD_MINB 5
 #endif
 
 namespace ope {

@@ -236,3 +236,123 @@ def summarize(res: dict) -> dict:
                 "p50_ms": float(np.nanpercentile(lat[sel], 50)), "p99_ms": float(np.nanpercentile(lat[sel], 99)),
                 "n": int(sel.sum())}
     return out
+
+
+def run_sustained(server: Server, pool: list[StreamRequest], rate: float, seconds: float, seed: int = 7,
+                  calib_share: float = 0.2, drain_s: float = 20.0) -> dict:
+    """A fresh Poisson stream at `rate` req/s for `seconds` of arrivals: each
+    arrival is a calibration with probability calib_share, else a reprice,
+    its contents drawn from `pool` (the server keeps no results between
+    requests, so repeated contents cost as much as new ones).  Reprices and
+    calibrations are collected by separate threads, so a saturated
+    calibration queue never delays the bookkeeping of reprices.  Whatever is
+    unfinished `drain_s` after the last arrival is cancelled and counted."""
+    rng = np.random.default_rng(seed)
+    rep = [r for r in pool if r.kind == 0]
+    cal = [r for r in pool if r.kind == 1]
+    n = max(1, int(round(rate * seconds)))
+    is_cal = (rng.uniform(size=n) < calib_share) if cal else np.zeros(n, bool)
+    which = np.where(is_cal, rng.integers(0, max(1, len(cal)), n), rng.integers(0, len(rep), n))
+    gaps = rng.exponential(1.0 / rate, n)
+    t_sub = np.full(n, np.nan)
+    lat = np.full(n, np.nan)
+    size = np.array([(cal[w] if c else rep[w]).size for c, w in zip(is_cal, which)])
+    queues = {0: [], 1: []}  # per kind: (index, rid) in submission order
+    cond = threading.Condition()
+    state = {"deadline": None, "unfinished": 0, "errors": []}
+    finished = {0: threading.Event(), 1: threading.Event()}
+
+    def collector(kind: int):
+        k = 0
+        while True:
+            with cond:
+                while k >= len(queues[kind]) and state["deadline"] is None:
+                    cond.wait(0.01)
+                if k >= len(queues[kind]):
+                    break
+                i, rid = queues[kind][k]
+                deadline = state["deadline"]
+            k += 1
+            timeout = -1.0 if deadline is None else max(0.0, 1e3 * (deadline - time.perf_counter()))
+            try:
+                _, ms = server.wait(rid, timeout)
+                lat[i] = ms
+            except OpeError as e:
+                if e.status == OPE_ERR_TIMEOUT:
+                    server.cancel(rid)
+                    try:
+                        server.wait(rid, 10000.0)
+                    except OpeError:
+                        pass
+                    with cond:
+                        state["unfinished"] += 1
+                else:
+                    state["errors"].append(str(e))
+        finished[kind].set()
+
+    threads = [threading.Thread(target=collector, args=(kd,), daemon=True) for kd in (0, 1)]
+    for th in threads:
+        th.start()
+    t0 = time.perf_counter()
+    t_next = t0
+    for i in range(n):
+        t_next += gaps[i]
+        now = time.perf_counter()
+        if t_next > now:
+            time.sleep(t_next - now)
+        r = cal[which[i]] if is_cal[i] else rep[which[i]]
+        t_sub[i] = time.perf_counter() - t0
+        if r.kind == 0:
+            rid = server.submit_price(MODEL_BATES, r.contracts, r.params)
+        else:
+            rid = server.submit_calibrate(MODEL_HESTON, r.contracts, r.iv, r.params)
+        with cond:
+            queues[r.kind].append((i, rid))
+            cond.notify_all()
+    t_arr = time.perf_counter() - t0
+    with cond:
+        state["deadline"] = time.perf_counter() + drain_s
+        cond.notify_all()
+    for kd in (0, 1):
+        finished[kd].wait()
+    return {"latency_ms": lat, "kind": is_cal.astype(int), "size": size, "t_submit": t_sub, "offered_rate": rate,
+            "arrival_s": t_arr, "wall_s": time.perf_counter() - t0, "unfinished": state["unfinished"],
+            "errors": state["errors"]}
+
+
+def summarize_sustained(res: dict) -> dict:
+    """Per stream: the arrival period, what was submitted and completed per
+    second of it, latency percentiles over the steady half (requests
+    submitted in the second half of the arrival period), by kind and by
+    reprice size, and the growth of the reprice latency across the run (the
+    median of the last quarter of submissions over that of the second
+    quarter: a queue that keeps growing shows here as a ratio well above 1)."""
+    lat, kind, size, ts = res["latency_ms"], res["kind"], res["size"], res["t_submit"]
+    T = res["arrival_s"]
+    done = np.isfinite(lat)
+    rep, cal = kind == 0, kind == 1
+    steady = ts >= 0.5 * T
+    out = {"offered_req_per_s": res["offered_rate"], "arrival_s": T, "wall_s": res["wall_s"],
+           "submitted_req_per_s": float(len(lat) / T), "requests": int(len(lat)),
+           "reprices_completed_per_s": float((rep & done).sum() / T),
+           "reprice_contracts_per_s": float(size[rep & done].sum() / T),
+           "calibrations_completed_per_s": float((cal & done).sum() / T),
+           "unfinished_after_drain": int(res["unfinished"]), "errors": len(res["errors"])}
+    for name, sel in (("reprice", rep), ("calibration", cal)):
+        sel = sel & done & steady
+        if sel.any():
+            out[name] = {"p50_ms": float(np.percentile(lat[sel], 50)), "p99_ms": float(np.percentile(lat[sel], 99)),
+                         "n": int(sel.sum())}
+    out["reprice_by_size"] = {}
+    for lo, hi in ((20, 100), (100, 500), (500, 2001)):
+        sel = rep & done & steady & (size >= lo) & (size < hi)
+        if sel.any():
+            out["reprice_by_size"][f"{lo}-{hi - 1}"] = {
+                "p50_ms": float(np.percentile(lat[sel], 50)), "p99_ms": float(np.percentile(lat[sel], 99)),
+                "n": int(sel.sum())}
+    q2 = rep & done & (ts >= 0.25 * T) & (ts < 0.5 * T)
+    q4 = rep & done & (ts >= 0.75 * T)
+    growth = float(np.median(lat[q4]) / np.median(lat[q2])) if q2.any() and q4.any() else None
+    out["reprice_latency_growth"] = growth
+    out["reprice_sustained"] = bool((rep & ~done).sum() == 0 and growth is not None and growth < 2.0)
+    return out
