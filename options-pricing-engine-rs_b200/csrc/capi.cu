@@ -10,6 +10,7 @@
 #include <mutex>
 #include <string>
 #include <tuple>
+#include <vector>
 
 #include "checked.cuh"
 #include "internal.h"
@@ -200,6 +201,77 @@ void* pinned_device_ptr(const void* host) {
     return a.type == cudaMemoryTypeHost ? a.devicePointer : nullptr;
 }
 
+// Calls from pageable host contracts of at least this many contracts take
+// the pipelined path below.
+constexpr size_t kPipelineMin = 262144;
+
+// Pageable host contracts (what a Rust Vec is), large calls: the contract copy
+// no longer precedes the whole launch.  The first eighth of the contracts is
+// copied and priced; the other seven eighths copy on the thread's copy stream
+// while that first launch runs, then price; each part's prices come back as
+// soon as its launch ends (from a pageable output the host waits for each;
+// into pinned memory the kernel writes them in place).  Two launches instead
+// of one cost one extra queue tail.  The parts split the contracts anywhere:
+// each gets its own rebased surface offsets (contract ranges clipped to the
+// part) and its parameter rows; every unit's arithmetic is that of a single
+// launch, so prices are bit-identical.  off_h == NULL: one parameter set
+// (d_par) for all contracts.  d_off2 holds room for n_surf + 3 offsets;
+// d_nb (NULL or 2n bisection counts) and out_nb follow the same parts.
+int price_pipelined(int model, const ope_contract* contracts, size_t n, const int64_t* off_h, size_t n_surf,
+                    const double* d_par, double tol, ope_contract* d_con, int64_t* d_off2, double* d_out,
+                    double* out_prices, double* k_out, int32_t* d_nb, int32_t* out_nb, void* scratch) {
+    ThreadCtx& c = tctx();
+    if (!c.copy_stream) OPE_CHECK(cudaStreamCreateWithFlags(&c.copy_stream, cudaStreamNonBlocking));
+    for (auto& e : c.pipe_ev)
+        if (!e) OPE_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    cudaStream_t st = c.stream, cs = c.copy_stream;
+    const int stride = param_stride(model);
+    const size_t c1 = n / 8;  // part A: [0, c1), part B: [c1, n)
+    // parts' surfaces and rebased offsets
+    size_t nsA = 1, nsB = 1, sB = 0;
+    std::vector<int64_t> offs;
+    if (off_h) {
+        const size_t sA_last = (size_t)(std::upper_bound(off_h, off_h + n_surf + 1, (int64_t)c1 - 1) - off_h) - 1;
+        sB = (size_t)(std::upper_bound(off_h, off_h + n_surf + 1, (int64_t)c1) - off_h) - 1;
+        nsA = sA_last + 1;
+        nsB = n_surf - sB;
+        offs.resize(nsA + 1 + nsB + 1);
+        for (size_t j = 0; j < nsA; ++j) offs[j] = std::min<int64_t>(off_h[j], (int64_t)c1);
+        offs[nsA] = (int64_t)c1;
+        for (size_t j = 0; j <= nsB; ++j) offs[nsA + 1 + j] = std::max<int64_t>(off_h[sB + j], (int64_t)c1) - (int64_t)c1;
+        OPE_CHECK(cudaMemcpyAsync(d_off2, offs.data(), offs.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+    }
+    const int64_t* offA = off_h ? d_off2 : nullptr;
+    const int64_t* offB = off_h ? d_off2 + nsA + 1 : nullptr;
+    const PriceScratch sc = carve_price_scratch(scratch, n);
+    double* oA = k_out ? k_out : d_out;
+    // part A: copy, then price
+    OPE_CHECK(cudaMemcpyAsync(d_con, contracts, c1 * sizeof(ope_contract), cudaMemcpyHostToDevice, cs));
+    OPE_CHECK(cudaEventRecord(c.pipe_ev[0], cs));
+    OPE_CHECK(cudaStreamWaitEvent(st, c.pipe_ev[0], 0));
+    OPE_TRY(launch_price_persistent(model, d_con, c1, offA, nsA, nullptr, d_par, tol, oA, sc, st, d_nb));
+    OPE_CHECK(cudaEventRecord(c.pipe_ev[2], st));
+    // part B: its copy overlaps part A's pricing
+    OPE_CHECK(cudaMemcpyAsync(d_con + c1, contracts + c1, (n - c1) * sizeof(ope_contract), cudaMemcpyHostToDevice,
+                              cs));
+    OPE_CHECK(cudaEventRecord(c.pipe_ev[1], cs));
+    OPE_CHECK(cudaStreamWaitEvent(st, c.pipe_ev[1], 0));
+    OPE_TRY(launch_price_persistent(model, d_con + c1, n - c1, offB, nsB, nullptr, d_par + sB * stride, tol, oA + c1,
+                                    sc, st, d_nb ? d_nb + 2 * c1 : nullptr));
+    OPE_CHECK(cudaEventRecord(c.pipe_ev[3], st));
+    // results: part A's while part B prices, then part B's
+    if (!k_out) {
+        OPE_CHECK(cudaStreamWaitEvent(cs, c.pipe_ev[2], 0));
+        OPE_CHECK(cudaMemcpyAsync(out_prices, d_out, c1 * sizeof(double), cudaMemcpyDeviceToHost, cs));
+        OPE_CHECK(cudaStreamWaitEvent(cs, c.pipe_ev[3], 0));
+        OPE_CHECK(cudaMemcpyAsync(out_prices + c1, d_out + c1, (n - c1) * sizeof(double), cudaMemcpyDeviceToHost, cs));
+    }
+    if (out_nb) OPE_CHECK(cudaMemcpyAsync(out_nb, d_nb, 2 * n * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    OPE_CHECK(cudaStreamSynchronize(cs));
+    OPE_CHECK(cudaStreamSynchronize(st));
+    return OPE_OK;
+}
+
 // Plain (one parameter set) pricing, host or device pointers.
 int batch_price(int32_t model, const ope_contract* contracts, size_t n, const void* params, double* out,
                 const ope_options* opts) {
@@ -229,11 +301,14 @@ int batch_price(int32_t model, const ope_contract* contracts, size_t n, const vo
     // contracts and prices in pinned host memory are used in place (zero-copy)
     const ope_contract* k_con = static_cast<const ope_contract*>(pinned_device_ptr(contracts));
     double* k_out = static_cast<double*>(pinned_device_ptr(out));
+    OPE_CHECK(cudaMemcpyAsync(d_par, params, stride * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    if (!k_con && n >= kPipelineMin)
+        return price_pipelined(model, contracts, n, nullptr, 1, d_par, tol, d_con, nullptr, d_out, out, k_out, nullptr,
+                               nullptr, scratch);
     if (!k_con) {
         OPE_CHECK(cudaMemcpyAsync(d_con, contracts, n * sizeof(ope_contract), cudaMemcpyHostToDevice, c.stream));
         k_con = d_con;
     }
-    OPE_CHECK(cudaMemcpyAsync(d_par, params, stride * sizeof(double), cudaMemcpyHostToDevice, c.stream));
     OPE_TRY(launch_price_persistent(model, k_con, n, nullptr, 1, nullptr, d_par, tol, k_out ? k_out : d_out,
                                     carve_price_scratch(scratch, n), c.stream));
     if (!k_out) OPE_CHECK(cudaMemcpyAsync(out, d_out, n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
@@ -621,7 +696,7 @@ int ope_price_surfaces_stats(int32_t model, const ope_contract* contracts, size_
     for (size_t s = 0; s < n_surf; ++s)
         if (surf_offsets[s + 1] < surf_offsets[s]) return set_error(OPE_ERR_INVALID_ARG, "surf_offsets not sorted");
     ThreadCtx& c = tctx();
-    const size_t b_con = align_up(n * sizeof(ope_contract), 256), b_off = align_up((n_surf + 1) * sizeof(int64_t), 256),
+    const size_t b_con = align_up(n * sizeof(ope_contract), 256), b_off = align_up((n_surf + 3) * sizeof(int64_t), 256),
                  b_par = align_up(n_surf * stride * sizeof(double), 256), b_out = align_up(n * sizeof(double), 256),
                  b_nb = out_bisections ? align_up(2 * n * sizeof(int32_t), 256) : 0;
     void* ws;
@@ -636,12 +711,15 @@ int ope_price_surfaces_stats(int32_t model, const ope_contract* contracts, size_
     // contracts and prices in pinned host memory are used in place (zero-copy)
     const ope_contract* k_con = static_cast<const ope_contract*>(pinned_device_ptr(contracts));
     double* k_out = static_cast<double*>(pinned_device_ptr(out_prices));
+    OPE_CHECK(cudaMemcpyAsync(d_par, params, n_surf * stride * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    if (!k_con && n >= kPipelineMin)
+        return price_pipelined(model, contracts, n, surf_offsets, n_surf, d_par, tol, d_con, d_off, d_out, out_prices,
+                               k_out, d_nb, out_bisections, scratch);
     if (!k_con) {
         OPE_CHECK(cudaMemcpyAsync(d_con, contracts, n * sizeof(ope_contract), cudaMemcpyHostToDevice, c.stream));
         k_con = d_con;
     }
     OPE_CHECK(cudaMemcpyAsync(d_off, surf_offsets, (n_surf + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, c.stream));
-    OPE_CHECK(cudaMemcpyAsync(d_par, params, n_surf * stride * sizeof(double), cudaMemcpyHostToDevice, c.stream));
     OPE_TRY(launch_price_persistent(model, k_con, n, d_off, n_surf, nullptr, d_par, tol, k_out ? k_out : d_out,
                                     carve_price_scratch(scratch, n), c.stream, d_nb));
     if (!k_out)

@@ -37,6 +37,10 @@ struct ThreadCtx {
     bool ws_recorded = false;
     bool ws_taken = false;
     int api_depth = 0;
+    // Copy stream and events of the pipelined pageable-host pricing path
+    // (created on first use with this thread's device).
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t pipe_ev[4] = {nullptr, nullptr, nullptr, nullptr};
 };
 
 ThreadCtx& tctx();

@@ -372,6 +372,48 @@ def test_pinned_host_buffers_zero_copy_equal_copy_path(ope):
     assert np.array_equal(got, ref[:256])
 
 
+def test_pipelined_pageable_calls_equal_pinned(ope):
+    """Large calls from pageable host buffers copy and price in two parts (the
+    second part's copy overlaps the first part's pricing): prices and
+    bisection counts equal the pinned (zero-copy, one launch) path bit for
+    bit -- with a surface straddling the split, with an empty surface at the
+    split, and for the one-parameter-set batch_bates."""
+    import torch
+
+    w = W.c3(n=1 << 18, per_surface=256, seed=29)
+    n = w.n
+
+    def pinned(a):
+        b = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True).numpy().view(a.dtype)
+        b[:] = a
+        return b
+
+    cases = []
+    off = w.surf_offsets.copy()
+    off[1:-1] += 77  # surfaces of 256 shifted: the split at n/8 falls inside a surface
+    off[-2] = min(off[-2], n)
+    cases.append((off, w.params))
+    # an empty surface exactly at the split
+    k = int(np.searchsorted(w.surf_offsets, n // 8))
+    off2 = np.concatenate([w.surf_offsets[:k], [n // 8], w.surf_offsets[k:]]).astype(np.int64)
+    off2[k] = n // 8
+    par2 = np.concatenate([w.params[:k], w.params[k:k + 1], w.params[k:]])
+    assert off2[k - 1] <= off2[k] <= off2[k + 1]
+    cases.append((off2, par2))
+    for off_, par_ in cases:
+        nb_pg, nb_pin = np.zeros(2 * n, np.int32), np.zeros(2 * n, np.int32)
+        pg = ope.price_surfaces(ope.MODEL_BATES, w.contracts, off_, par_, tol=w.tol, bisections=nb_pg)
+        pin_out = pinned(np.zeros(n))
+        ope.price_surfaces(ope.MODEL_BATES, pinned(w.contracts), off_, par_, tol=w.tol, out=pin_out,
+                           bisections=nb_pin)
+        assert np.array_equal(pg, pin_out) and np.array_equal(nb_pg, nb_pin)
+    # one parameter set: the drop-in batch_bates on 2^18 pageable contracts
+    got = ope.batch_bates(w.contracts, w.params[0], tol=w.tol)
+    ref = ope.price_surfaces(ope.MODEL_BATES, pinned(w.contracts), np.array([0, n], np.int64), w.params[:1],
+                             tol=w.tol)
+    assert np.array_equal(got, ref)
+
+
 def test_workspace_limit_fails_cleanly_and_recovers(ope):
     """Injected allocation failure without a GPU fault: under a 1 MiB workspace
     cap a call that needs more fails with OPE_ERR_OUT_OF_MEMORY before
