@@ -204,6 +204,31 @@ void* pinned_device_ptr(const void* host) {
 // Calls from pageable host contracts of at least this many contracts take
 // the pipelined path below.
 constexpr size_t kPipelineMin = 262144;
+// Calls from pageable host contracts of at most this many contracts stage them
+// through the thread's pinned buffer (a host memcpy) and let the kernel read
+// them and write the prices there in place (zero-copy), instead of a staged
+// pageable copy each way around the launch: a small call's time is mostly
+// these fixed costs.
+constexpr size_t kStagedMax = 16384;
+
+// The staged small-call setup: contracts copied into the pinned buffer
+// (*k_con points at them); *h_out is the pinned slot for the prices (NULL
+// when the caller's output is pinned already, *k_out).
+int stage_small(const ope_contract* contracts, size_t n, const ope_contract** k_con, double** k_out,
+                double** h_out) {
+    const size_t b_con = align_up(n * sizeof(ope_contract), 256);
+    void* pin;
+    OPE_TRY(ensure_pinned(b_con + align_up(n * sizeof(double), 256), &pin));
+    std::memcpy(pin, contracts, n * sizeof(ope_contract));
+    *k_con = static_cast<const ope_contract*>(pinned_device_ptr(pin));
+    *h_out = nullptr;
+    if (!*k_out) {
+        *h_out = reinterpret_cast<double*>(static_cast<char*>(pin) + b_con);
+        *k_out = static_cast<double*>(pinned_device_ptr(*h_out));
+    }
+    if (!*k_con || !*k_out) return set_error(OPE_ERR_DEVICE, "pinned staging buffer is not device-accessible");
+    return OPE_OK;
+}
 
 // Pageable host contracts (what a Rust Vec is), large calls: the contract copy
 // no longer precedes the whole launch.  The first eighth of the contracts is
@@ -305,6 +330,15 @@ int batch_price(int32_t model, const ope_contract* contracts, size_t n, const vo
     if (!k_con && n >= kPipelineMin)
         return price_pipelined(model, contracts, n, nullptr, 1, d_par, tol, d_con, nullptr, d_out, out, k_out, nullptr,
                                nullptr, scratch);
+    double* h_out = nullptr;
+    if (!k_con && n <= kStagedMax) {
+        OPE_TRY(stage_small(contracts, n, &k_con, &k_out, &h_out));
+        OPE_TRY(launch_price_persistent(model, k_con, n, nullptr, 1, nullptr, d_par, tol, k_out,
+                                        carve_price_scratch(scratch, n), c.stream));
+        OPE_CHECK(cudaStreamSynchronize(c.stream));
+        if (h_out) std::memcpy(out, h_out, n * sizeof(double));
+        return OPE_OK;
+    }
     if (!k_con) {
         OPE_CHECK(cudaMemcpyAsync(d_con, contracts, n * sizeof(ope_contract), cudaMemcpyHostToDevice, c.stream));
         k_con = d_con;
@@ -715,6 +749,8 @@ int ope_price_surfaces_stats(int32_t model, const ope_contract* contracts, size_
     if (!k_con && n >= kPipelineMin)
         return price_pipelined(model, contracts, n, surf_offsets, n_surf, d_par, tol, d_con, d_off, d_out, out_prices,
                                k_out, d_nb, out_bisections, scratch);
+    double* h_out = nullptr;
+    if (!k_con && n <= kStagedMax) OPE_TRY(stage_small(contracts, n, &k_con, &k_out, &h_out));
     if (!k_con) {
         OPE_CHECK(cudaMemcpyAsync(d_con, contracts, n * sizeof(ope_contract), cudaMemcpyHostToDevice, c.stream));
         k_con = d_con;
@@ -727,6 +763,7 @@ int ope_price_surfaces_stats(int32_t model, const ope_contract* contracts, size_
     if (out_bisections)
         OPE_CHECK(cudaMemcpyAsync(out_bisections, d_nb, 2 * n * sizeof(int32_t), cudaMemcpyDeviceToHost, c.stream));
     OPE_CHECK(cudaStreamSynchronize(c.stream));
+    if (h_out) std::memcpy(out_prices, h_out, n * sizeof(double));
     return OPE_OK;
 }
 
