@@ -271,23 +271,27 @@ def run_sustained(server: Server, pool: list[StreamRequest], rate: float, second
                 if k >= len(queues[kind]):
                     break
                 i, rid = queues[kind][k]
-                deadline = state["deadline"]
             k += 1
-            timeout = -1.0 if deadline is None else max(0.0, 1e3 * (deadline - time.perf_counter()))
-            try:
-                _, ms = server.wait(rid, timeout)
-                lat[i] = ms
-            except OpeError as e:
-                if e.status == OPE_ERR_TIMEOUT:
-                    server.cancel(rid)
-                    try:
-                        server.wait(rid, 10000.0)
-                    except OpeError:
-                        pass
-                    with cond:
-                        state["unfinished"] += 1
-                else:
-                    state["errors"].append(str(e))
+            while True:  # bounded waits: the drain deadline is re-read between them
+                deadline = state["deadline"]
+                timeout = 50.0 if deadline is None else max(0.0, 1e3 * (deadline - time.perf_counter()))
+                try:
+                    _, ms = server.wait(rid, timeout)
+                    lat[i] = ms
+                    break
+                except OpeError as e:
+                    if e.status != OPE_ERR_TIMEOUT:
+                        state["errors"].append(str(e))
+                        break
+                    if deadline is not None and time.perf_counter() >= deadline:
+                        server.cancel(rid)
+                        try:
+                            server.wait(rid, 10000.0)
+                        except OpeError:
+                            pass
+                        with cond:
+                            state["unfinished"] += 1
+                        break
         finished[kind].set()
 
     threads = [threading.Thread(target=collector, args=(kd,), daemon=True) for kd in (0, 1)]
