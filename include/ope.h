@@ -388,6 +388,15 @@ typedef struct {
     int32_t warps_per_block; /* 1, 2 or 4 */
     int32_t deepest_first;   /* 1: queue deepest-first, 0: input order */
     double occupancy;        /* share of the resident blocks per SM, (0, 1] */
+    int32_t per_unit;        /* contracts per work unit, 0..32.  1: one.  From 2, a warp integrates blocks
+                              * of that many consecutive contracts, and a run of contracts of one parameter
+                              * set with the same expiry and rate (the strikes of one expiry of a surface
+                              * laid out expiry by expiry) evaluates the characteristic function once per
+                              * panel for the whole run (4 warps, input order).  0 (the default):
+                              * automatic -- a call of 32,768 contracts or more counts its runs on the
+                              * device and takes blocks of 16 when they average 4 contracts or more.
+                              * Prices are bit-identical in every mode. */
+    int32_t reserved;        /* 0 */
 } ope_launch_shape;
 typedef struct {
     uint64_t max_contracts;  /* the class: calls of at most this many contracts (the last: all larger) */
@@ -399,12 +408,17 @@ typedef struct {
 #define OPE_TUNE_QUICK 1u    /* ope_autotune flag: measure the classes up to 2^17 contracts only (the
                               * larger ones keep the default shape) */
 int ope_autotune(int32_t model, uint32_t flags, ope_tune_entry* out_entries);
+/* Contracts per unit that this thread's last plain pricing call launched
+ * with (1: one per unit; for an automatic launch, the run probe's choice --
+ * read after that call's work, so it waits for it).  Ask before the thread's
+ * next call. */
+int ope_last_per_unit(int32_t* out_per_unit);
 int ope_set_autotune(int32_t enabled);
 int ope_get_tune_table(int32_t model, ope_tune_entry* out_entries, int32_t* out_tuned);
 /* Installs OPE_TUNE_CLASSES entries (e.g. a table saved from
  * ope_get_tune_table in an earlier process) as the current device's tuned
  * table for `model`; each shape must be valid (1, 2 or 4 warps; 0 or 1;
- * occupancy in (0, 1]), max_contracts is ignored. */
+ * occupancy in (0, 1]; per_unit 0..32), max_contracts is ignored. */
 int ope_set_tune_table(int32_t model, const ope_tune_entry* entries);
 
 /* No reference twin (diagnostic of heston.rs:193-212 adaptive_gk): the step

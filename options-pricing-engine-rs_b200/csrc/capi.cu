@@ -104,6 +104,7 @@ int ensure_workspace(size_t bytes, void** out, cudaStream_t st) {
             OPE_CHECK(cudaFreeAsync(c.ws, st));
             c.ws = nullptr;
             c.ws_bytes = 0;
+            c.last_probe = nullptr;  // lived in the old block
         }
         OPE_CHECK(cudaMallocAsync(&c.ws, want, st));
         c.ws_bytes = want;
@@ -241,10 +242,12 @@ int stage_small(const ope_contract* contracts, size_t n, const ope_contract** k_
 // part) and its parameter rows; every unit's arithmetic is that of a single
 // launch, so prices are bit-identical.  off_h == NULL: one parameter set
 // (d_par) for all contracts.  d_off2 holds room for n_surf + 3 offsets;
-// d_nb (NULL or 2n bisection counts) and out_nb follow the same parts.
+// d_nb (NULL or 2n bisection counts) and out_nb follow the same parts;
+// scratch holds price_scratch_bytes(n) bytes and run_bytes of run cache.
 int price_pipelined(int model, const ope_contract* contracts, size_t n, const int64_t* off_h, size_t n_surf,
                     const double* d_par, double tol, ope_contract* d_con, int64_t* d_off2, double* d_out,
-                    double* out_prices, double* k_out, int32_t* d_nb, int32_t* out_nb, void* scratch) {
+                    double* out_prices, double* k_out, int32_t* d_nb, int32_t* out_nb, void* scratch,
+                    size_t run_bytes) {
     ThreadCtx& c = tctx();
     if (!c.copy_stream) OPE_CHECK(cudaStreamCreateWithFlags(&c.copy_stream, cudaStreamNonBlocking));
     for (auto& e : c.pipe_ev)
@@ -268,7 +271,7 @@ int price_pipelined(int model, const ope_contract* contracts, size_t n, const in
     }
     const int64_t* offA = off_h ? d_off2 : nullptr;
     const int64_t* offB = off_h ? d_off2 + nsA + 1 : nullptr;
-    const PriceScratch sc = carve_price_scratch(scratch, n);
+    const PriceScratch sc = carve_price_scratch(scratch, n, run_bytes);
     double* oA = k_out ? k_out : d_out;
     // part A: copy, then price
     OPE_CHECK(cudaMemcpyAsync(d_con, contracts, c1 * sizeof(ope_contract), cudaMemcpyHostToDevice, cs));
@@ -310,14 +313,16 @@ int batch_price(int32_t model, const ope_contract* contracts, size_t n, const vo
     const int stride = param_stride(model);
     if (device_ptrs(opts)) {
         void* ws;
-        OPE_TRY(ensure_workspace(price_scratch_bytes(n), &ws, user_stream(opts)));
+        const size_t b_run = price_run_bytes(model, n);
+        OPE_TRY(ensure_workspace(price_scratch_bytes(n) + b_run, &ws, user_stream(opts)));
         return launch_price_persistent(model, contracts, n, nullptr, 1, nullptr, static_cast<const double*>(params),
-                                       tol, out, carve_price_scratch(ws, n), user_stream(opts));
+                                       tol, out, carve_price_scratch(ws, n, b_run), user_stream(opts));
     }
     ThreadCtx& c = tctx();
-    const size_t b_con = align_up(n * sizeof(ope_contract), 256), b_par = 256, b_out = align_up(n * sizeof(double), 256);
+    const size_t b_con = align_up(n * sizeof(ope_contract), 256), b_par = 256, b_out = align_up(n * sizeof(double), 256),
+                 b_run = price_run_bytes(model, n);
     void* ws;
-    OPE_TRY(ensure_workspace(b_con + b_par + b_out + price_scratch_bytes(n), &ws, c.stream));
+    OPE_TRY(ensure_workspace(b_con + b_par + b_out + price_scratch_bytes(n) + b_run, &ws, c.stream));
     char* p = static_cast<char*>(ws);
     ope_contract* d_con = reinterpret_cast<ope_contract*>(p);
     double* d_par = reinterpret_cast<double*>(p + b_con);
@@ -329,12 +334,12 @@ int batch_price(int32_t model, const ope_contract* contracts, size_t n, const vo
     OPE_CHECK(cudaMemcpyAsync(d_par, params, stride * sizeof(double), cudaMemcpyHostToDevice, c.stream));
     if (!k_con && n >= kPipelineMin)
         return price_pipelined(model, contracts, n, nullptr, 1, d_par, tol, d_con, nullptr, d_out, out, k_out, nullptr,
-                               nullptr, scratch);
+                               nullptr, scratch, b_run);
     double* h_out = nullptr;
     if (!k_con && n <= kStagedMax) {
         OPE_TRY(stage_small(contracts, n, &k_con, &k_out, &h_out));
         OPE_TRY(launch_price_persistent(model, k_con, n, nullptr, 1, nullptr, d_par, tol, k_out,
-                                        carve_price_scratch(scratch, n), c.stream));
+                                        carve_price_scratch(scratch, n, b_run), c.stream));
         OPE_CHECK(cudaStreamSynchronize(c.stream));
         if (h_out) std::memcpy(out, h_out, n * sizeof(double));
         return OPE_OK;
@@ -344,7 +349,7 @@ int batch_price(int32_t model, const ope_contract* contracts, size_t n, const vo
         k_con = d_con;
     }
     OPE_TRY(launch_price_persistent(model, k_con, n, nullptr, 1, nullptr, d_par, tol, k_out ? k_out : d_out,
-                                    carve_price_scratch(scratch, n), c.stream));
+                                    carve_price_scratch(scratch, n, b_run), c.stream));
     if (!k_out) OPE_CHECK(cudaMemcpyAsync(out, d_out, n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
     OPE_CHECK(cudaStreamSynchronize(c.stream));
     return OPE_OK;
@@ -720,10 +725,11 @@ int ope_price_surfaces_stats(int32_t model, const ope_contract* contracts, size_
     const int stride = param_stride(model);
     if (device_ptrs(opts)) {
         void* ws;
-        OPE_TRY(ensure_workspace(price_scratch_bytes(n), &ws, user_stream(opts)));
+        const size_t b_run = price_run_bytes(model, n);
+        OPE_TRY(ensure_workspace(price_scratch_bytes(n) + b_run, &ws, user_stream(opts)));
         return launch_price_persistent(model, contracts, n, surf_offsets, n_surf, nullptr,
-                                       static_cast<const double*>(params), tol, out_prices, carve_price_scratch(ws, n),
-                                       user_stream(opts), out_bisections);
+                                       static_cast<const double*>(params), tol, out_prices,
+                                       carve_price_scratch(ws, n, b_run), user_stream(opts), out_bisections);
     }
     if (surf_offsets[0] != 0 || surf_offsets[n_surf] != (int64_t)n)
         return set_error(OPE_ERR_INVALID_ARG, "surf_offsets must start at 0 and end at n");
@@ -732,9 +738,9 @@ int ope_price_surfaces_stats(int32_t model, const ope_contract* contracts, size_
     ThreadCtx& c = tctx();
     const size_t b_con = align_up(n * sizeof(ope_contract), 256), b_off = align_up((n_surf + 3) * sizeof(int64_t), 256),
                  b_par = align_up(n_surf * stride * sizeof(double), 256), b_out = align_up(n * sizeof(double), 256),
-                 b_nb = out_bisections ? align_up(2 * n * sizeof(int32_t), 256) : 0;
+                 b_nb = out_bisections ? align_up(2 * n * sizeof(int32_t), 256) : 0, b_run = price_run_bytes(model, n);
     void* ws;
-    OPE_TRY(ensure_workspace(b_con + b_off + b_par + b_out + b_nb + price_scratch_bytes(n), &ws, c.stream));
+    OPE_TRY(ensure_workspace(b_con + b_off + b_par + b_out + b_nb + price_scratch_bytes(n) + b_run, &ws, c.stream));
     char* p = static_cast<char*>(ws);
     ope_contract* d_con = reinterpret_cast<ope_contract*>(p);
     int64_t* d_off = reinterpret_cast<int64_t*>(p + b_con);
@@ -748,7 +754,7 @@ int ope_price_surfaces_stats(int32_t model, const ope_contract* contracts, size_
     OPE_CHECK(cudaMemcpyAsync(d_par, params, n_surf * stride * sizeof(double), cudaMemcpyHostToDevice, c.stream));
     if (!k_con && n >= kPipelineMin)
         return price_pipelined(model, contracts, n, surf_offsets, n_surf, d_par, tol, d_con, d_off, d_out, out_prices,
-                               k_out, d_nb, out_bisections, scratch);
+                               k_out, d_nb, out_bisections, scratch, b_run);
     double* h_out = nullptr;
     if (!k_con && n <= kStagedMax) OPE_TRY(stage_small(contracts, n, &k_con, &k_out, &h_out));
     if (!k_con) {
@@ -757,7 +763,7 @@ int ope_price_surfaces_stats(int32_t model, const ope_contract* contracts, size_
     }
     OPE_CHECK(cudaMemcpyAsync(d_off, surf_offsets, (n_surf + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, c.stream));
     OPE_TRY(launch_price_persistent(model, k_con, n, d_off, n_surf, nullptr, d_par, tol, k_out ? k_out : d_out,
-                                    carve_price_scratch(scratch, n), c.stream, d_nb));
+                                    carve_price_scratch(scratch, n, b_run), c.stream, d_nb));
     if (!k_out)
         OPE_CHECK(cudaMemcpyAsync(out_prices, d_out, n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
     if (out_bisections)

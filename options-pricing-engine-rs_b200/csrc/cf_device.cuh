@@ -4,7 +4,7 @@
 // (fast_csqrt), heston.rs:220-227 (the [0,inf) -> [0,1] substitution),
 // bates.rs:65-83 (bates_integrand, jump_cf).
 //
-// One call of `node_value` evaluates gk_integrate's g(t) at one GK node:
+// `node_cf` + `node_finish` evaluate gk_integrate's g(t) at one GK node:
 // u = (1-t)/t, f(u)/t^2, non-finite -> 0.  The Albrecher stable CF is
 // evaluated with its per-contract constants hoisted into CfConsts.  The
 // three exponential factors the reference multiplies together per node
@@ -21,6 +21,14 @@
 // CF(-i) evaluated with the reference's own operation sequence, so the
 // degenerate cases (CF(-i) = 0, inf or NaN) zero the P1 integrand exactly as
 // the reference's division does.
+//
+// Of Z only the phase u x depends on the strike (x = ln(S/K)); the rest is a
+// function of the node, the expiry, the rate, the parameters and the
+// integral.  So the evaluation is split: node_cf gives the strike-free part
+// (W = e^{Re Z}/((1-t)t), Im Z without u x, and u), node_finish adds one
+// strike's phase and forms the value.  Contracts of one surface that share
+// an expiry and a rate share node_cf's values at every panel they both
+// bisect (the run cache of quadrature.cuh).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -380,9 +388,21 @@ __device__ __forceinline__ double node_u(double omt, double tn, double itt) {
     return fma(fma(-u0, tn, omt), yt, u0);
 }
 
-// gk_integrate's g(t) (heston.rs:221-227) with the merged-exponent integrand.
+// The strike-free part of a node (heston.rs:221-227 with the merged-exponent
+// integrand): W = e^{Re Z} / ((1 - t) t), or NaN where the reference's g(t) is
+// 0 whatever the strike (t <= 0, u < 1e-12); A = Im Z - (u x mod 2 pi); u.
+struct NodeCf {
+    double w, a, u;
+};
+
+// u of a node alone, as node_cf computes it (bit for bit).
+__device__ __forceinline__ double node_u_of(double tn) {
+    const double omt = 1.0 - tn;
+    return node_u(omt, tn, rcp_nr(omt * tn));
+}
+
 template <bool BATES>
-__device__ __forceinline__ double node_value(const CfConsts& C, double tn) {
+__device__ __forceinline__ NodeCf node_cf(const CfConsts& C, double tn) {
     const double omt = 1.0 - tn;
     const double itt = rcp_nr(omt * tn);  // 1 / ((1 - t) t)
     const double u = node_u(omt, tn, itt);    // (1 - t) / t
@@ -439,19 +459,8 @@ __device__ __forceinline__ double node_value(const CfConsts& C, double tn) {
     // Ch = (xi - d) T - 2 Log A
     const double Cr = fma(amr, C.t, -2.0 * lr);
     const double Ci = fma(ami, C.t, -2.0 * li);
-    // The phase of e^{iux} (heston.rs:107), u x rounded as the reference
-    // rounds it, reduced modulo 2 pi without loss (Cody and Waite's argument
-    // reduction, 2 pi split into two doubles and the products taken exactly by
-    // FMA: |u x - n 2 pi| < 4 makes the first step exact), so that adding the
-    // CF's own phase costs an ulp of a number below 4 however large u x is.
-    // The reference adds the two phases exactly too, through the complex
-    // product e^{iux} CF (an unreduced sum would lose ulp(u x), 1e-9 at
-    // u x = 1e7, on short-dated deep-wing contracts).
-    const double ux = __dmul_rn(u, C.x);
-    const double nq = rint(ux * 0.15915494309189535);  // 1 / (2 pi)
-    const double uxr = fma(-nq, 2.4492935982947064e-16, fma(-nq, 6.283185307179586, ux));
     double zre = fma(C.kts, Cr, fma(C.v0s, Dr, C.z0re));
-    double zim = fma(C.kts, Ci, fma(C.v0s, Di, fma(C.rt, u, C.z0im))) + uxr;
+    double zim = fma(C.kts, Ci, fma(C.v0s, Di, fma(C.rt, u, C.z0im)));
     if (BATES) {
         double js, jc;
         sincos(C.jmu * u, &js, &jc);
@@ -459,10 +468,26 @@ __device__ __forceinline__ double node_value(const CfConsts& C, double tn) {
         zre += fma(je, jc, C.jre0);
         zim += fma(je, js, -C.ltc * u);
     }
-    // Im(e^Z) / u / t^2 = e^{Re Z} sin(Im Z) / ((1 - t) t)
-    const double v = exp(zre) * sin(zim) * itt;
-    const bool ok = (tn > 0.0) && (u >= 1e-12) && isfinite(v);
-    return ok ? v : 0.0;
+    const bool live = (tn > 0.0) && (u >= 1e-12);
+    return NodeCf{live ? __dmul_rn(exp(zre), itt) : __longlong_as_double(0x7ff8000000000000ll), zim, u};
+}
+
+// One strike's node value from the strike-free part: Im(e^Z) / u / t^2 =
+// e^{Re Z} sin(Im Z) / ((1 - t) t) = sin(A + phase) W, non-finite -> 0.
+// The phase of e^{iux} (heston.rs:107): u x rounded as the reference rounds
+// it, reduced modulo 2 pi without loss (Cody and Waite's argument reduction,
+// 2 pi split into two doubles and the products taken exactly by FMA:
+// |u x - n 2 pi| < 4 makes the first step exact), so that adding the CF's own
+// phase costs an ulp of a number below 4 however large u x is.  The
+// reference adds the two phases exactly too, through the complex product
+// e^{iux} CF (an unreduced sum would lose ulp(u x), 1e-9 at u x = 1e7, on
+// short-dated deep-wing contracts).
+__device__ __forceinline__ double node_finish(double x, const NodeCf& n) {
+    const double ux = __dmul_rn(n.u, x);
+    const double nq = rint(ux * 0.15915494309189535);  // 1 / (2 pi)
+    const double uxr = fma(-nq, 2.4492935982947064e-16, fma(-nq, 6.283185307179586, ux));
+    const double v = __dmul_rn(sin(__dadd_rn(n.a, uxr)), n.w);
+    return isfinite(v) ? v : 0.0;
 }
 
 }  // namespace ope

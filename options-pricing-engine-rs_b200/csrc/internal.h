@@ -41,6 +41,12 @@ struct ThreadCtx {
     // (created on first use with this thread's device).
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t pipe_ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    // contracts per unit of this thread's last plain pricing launch: fixed
+    // (last_per_unit), or the run probe's choice in the workspace word
+    // last_probe (on last_probe_stream) for an automatic launch
+    int last_per_unit = 1;
+    const unsigned long long* last_probe = nullptr;
+    cudaStream_t last_probe_stream = nullptr;
 };
 
 ThreadCtx& tctx();
@@ -113,9 +119,19 @@ struct PriceScratch {
     uint32_t* order = nullptr;     // n   queue position -> contract
     uint32_t* bucket = nullptr;    // n   depth bucket of each contract
     unsigned int* hist = nullptr;  // 2 x 64 bucket counts and fill counters
+    // run cache of the run kernel (optional; run_cache_bytes() bytes): without
+    // it a launch takes one contract per unit whatever its shape asks
+    void* runcache = nullptr;
+    size_t runcache_bytes = 0;
 };
 size_t price_scratch_bytes(size_t n);
 PriceScratch carve_price_scratch(void* base, size_t n);
+// The same with the run cache (run_bytes of it, 0: none) right after the
+// price_scratch_bytes(n) bytes; price_run_bytes(model, n): the run cache a
+// plain launch of n contracts wants under the current launch shape (0 or
+// run_cache_bytes()).  Callers size and carve with one value of it.
+PriceScratch carve_price_scratch(void* base, size_t n, size_t run_bytes);
+size_t price_run_bytes(int model, size_t n);
 
 // Launch shape of a plain pricing launch: warps per block (each warp one
 // integral, so warps / 2 contracts per block) of the persistent grid, whether
@@ -128,7 +144,17 @@ struct LaunchShape {
     int warps = 4;
     int deepest_first = 0;
     double occupancy = 1.0;
+    // contracts per unit: 1 = one contract per unit (k_price_persistent);
+    // 2..32 = blocks of that many consecutive contracts per warp, runs of
+    // equal (parameter set, expiry, rate) sharing a run cache (k_price_runs,
+    // input order); 0 = automatic: a call of 32,768 contracts or more probes
+    // its contracts on the device and takes the run kernel when its runs
+    // average 4 contracts or more
+    int per_unit = 0;
 };
+// Bytes of the run cache for the current device (every warp the run
+// kernel's grid can hold); 0 without a device.
+size_t run_cache_bytes();
 constexpr int kTuneClasses = 16;  // OPE_TUNE_CLASSES
 // Size classes of the tuning table: calls of at most kTuneClassMax[i]
 // contracts (64, 128, ..., 2^20; the last class: all larger calls).

@@ -34,11 +34,30 @@
 #ifndef OPE_KERNEL_MINB_HESTON
 #define OPE_KERNEL_MINB_HESTON 8
 #endif
+// The same for the run kernel (both models).
+#ifndef OPE_RUNS_MINB
+#define OPE_RUNS_MINB 8
+#endif
 
 namespace ope {
 
 namespace {
 constexpr int kOrderBuckets = 64;
+// Run cache entries per warp (panels of one run), and warps per SM it is
+// sized for (the 64-register budget holds at most 32).
+#ifndef OPE_RUN_CACHE_ENTRIES
+#define OPE_RUN_CACHE_ENTRIES 128
+#endif
+constexpr int kRunCacheEntries = OPE_RUN_CACHE_ENTRIES;
+constexpr int kRunWarpsPerSm = 32;
+// Automatic launches (per_unit 0): calls of at least kRunsMinContracts
+// contracts probe for runs (k_run_probe), which picks kRunsMinPerUnit to
+// kRunsMaxPerUnit contracts per unit, or the per-contract kernel.
+constexpr size_t kRunsMinContracts = 32768;
+constexpr int kRunsMinPerUnit = 4;
+constexpr int kRunsMaxPerUnit = 16;
+constexpr int kRunsUnitsPerWarp = 24;
+constexpr size_t kRunCacheWarpBytes = (size_t)kRunCacheEntries * (2 * 16 * sizeof(double) + sizeof(uint32_t));
 }
 
 // Layout: integ (2n doubles) | done (n) | head (256 B) | hist (2 x kOrderBuckets
@@ -51,6 +70,20 @@ size_t price_scratch_bytes(size_t n) {
 
 size_t panel_sink_bytes(size_t n, int n_slots) {
     return align_up(2 * n * n_slots * 2 * kMaxPanels * sizeof(double), 256) + align_up(2 * n * n_slots * sizeof(int32_t), 256);
+}
+
+PriceScratch carve_price_scratch(void* base, size_t n, size_t run_bytes) {
+    PriceScratch s = carve_price_scratch(base, n);
+    if (run_bytes) {
+        s.runcache = static_cast<char*>(base) + price_scratch_bytes(n);
+        s.runcache_bytes = run_bytes;
+    }
+    return s;
+}
+
+size_t price_run_bytes(int model, size_t n) {
+    const int pu = price_shape(model, n).per_unit;
+    return (pu > 1 || (pu == 0 && n >= kRunsMinContracts)) ? run_cache_bytes() : 0;
 }
 
 PanelSink carve_panel_sink(void* base, size_t n, int n_slots, const int32_t* slot) {
@@ -110,11 +143,12 @@ __device__ __forceinline__ ContractView load_contract(const ope_contract* con, l
 // contract, write the price.  SAVE: also store the final live-panel list
 // and the bisection count in `sink` (slot `slot`), for the adjoint's backward
 // pass.
-template <bool BATES, bool SAVE>
+// CACHED: through the run cache `rc` (the run kernel).
+template <bool BATES, bool SAVE, bool CACHED = false>
 __device__ __forceinline__ void run_unit(long long c, int which, const ope_contract* con, const double* p,
                                          double tol, double* out, double* integ, unsigned int* done,
                                          int32_t* nbis_out, const PanelSink& sink, int slot, PanelStore& L,
-                                         CfConsts& Cs, int lane, const LaneRule& R) {
+                                         CfConsts& Cs, int lane, const LaneRule& R, RunCacheWarp* rc = nullptr) {
     {
         const ContractView v = load_contract(con, c, lane);
         double pl[8];
@@ -127,7 +161,7 @@ __device__ __forceinline__ void run_unit(long long c, int which, const ope_contr
     }
     const CfConsts& C = Cs;
     int nb;
-    const double I = gk_integrate_warp<BATES>(C, tol, L, lane, R, &nb);
+    const double I = gk_integrate_warp<BATES, CACHED>(C, tol, L, lane, R, &nb, NoTrace(), rc);
     if (SAVE) {
         const size_t idx = (size_t)(2 * c + which) * sink.n_slots + slot;
         double* dst = sink.panels + idx * (2 * kMaxPanels);
@@ -212,6 +246,142 @@ __global__ void __launch_bounds__(WARPS * 32, (BATES ? OPE_KERNEL_MINB_BATES : O
         if (SAVE && !ope_check(slot >= 0 && slot < sink.n_slots, CHK_SLOT)) slot = 0;
         run_unit<BATES, SAVE>(c, (int)(unit & 1), con, params + s * stride, tol, out, integ, done, nbis_out,
                               sink, slot, smem_panels[warp], s_consts[warp], lane, R);
+    }
+}
+
+// The run kernel: the queue hands out blocks of `per_unit` consecutive
+// contracts (unit 2b + which: integral `which` of block b), and one warp
+// integrates a block's contracts one after another.  A block splits into runs
+// -- maximal stretches of contracts with the same parameter set, expiry and
+// rate, whose integrands differ only in the phase u ln(S/K) -- and each run of
+// two or more contracts shares one run cache (quadrature.cuh), so a surface
+// laid out expiry by expiry evaluates the characteristic function once per
+// panel and expiry instead of once per panel and strike.  A run never
+// reaches across blocks; contracts alone in their run are integrated
+// uncached.  Prices are bit-identical to k_price_persistent's.
+struct RunCacheMem {
+    double* vals;     // per warp of the grid: [2][cap][16] (w, a)
+    uint32_t* child;  // per warp of the grid: [cap]
+    int cap;
+};
+
+template <bool BATES, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, OPE_RUNS_MINB * 4 / WARPS)
+    k_price_runs(const ope_contract* __restrict__ con, long long n, const int64_t* __restrict__ surf_off,
+                 long long n_surf, const int32_t* __restrict__ param_idx, const double* __restrict__ params,
+                 double tol, double* __restrict__ out, double* integ, unsigned int* done, unsigned long long* head,
+                 int32_t* nbis_out, int per_unit_arg, RunCacheMem mem) {
+    extern __shared__ PanelStore smem_panels[];  // [WARPS], then the entry slots [WARPS][kMaxPanels]
+    __shared__ CfConsts s_consts[WARPS];
+    const unsigned FULL = 0xffffffffu;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const LaneRule R = lane_rule(lane);
+    const int stride = BATES ? 8 : 5;
+    const size_t gw = (size_t)blockIdx.x * WARPS + warp;
+    RunCacheWarp rc;
+    rc.cap = mem.cap;
+    rc.w = mem.vals + gw * 2 * (size_t)mem.cap * 16;
+    rc.a = rc.w + (size_t)mem.cap * 16;
+    rc.child = mem.child + gw * (size_t)mem.cap;
+    rc.slot = reinterpret_cast<uint16_t*>(smem_panels + WARPS) + warp * kMaxPanels;
+    rc.n_alloc = 0;
+    rc.on = false;
+    // contracts per unit: the launch's, or (0) the run probe's choice; with
+    // no choice (the probe kept the per-contract kernel) the queue is closed
+    int per_unit = per_unit_arg;
+    if (per_unit <= 0) per_unit = (int)min(__ldcg(head + 9), 32ull);  // head + 9 = the probe's head[25]
+    if (per_unit <= 0) per_unit = 1;
+    const unsigned long long n_blocks = ((unsigned long long)n + per_unit - 1) / per_unit;
+    const PanelSink none{nullptr, nullptr, nullptr, 1};
+    while (true) {
+        unsigned long long unit = 0;
+        if (lane == 0) unit = atomicAdd(head, 1ull);
+        unit = __shfl_sync(FULL, unit, 0);
+        if (unit >= 2ull * n_blocks) {
+            run_cache_discard(rc, lane);
+            break;
+        }
+        const long long c0 = (long long)(unit >> 1) * per_unit;
+        const int which = (int)(unit & 1);
+        const int cnt = (int)min((long long)per_unit, n - c0);
+        // run keys of the block's contracts, one lane each; a contract starts
+        // a run when its key differs from its predecessor's
+        long long ps = -1, tb = 0, rb = 0;
+        if (lane < cnt) {
+            ps = param_set(param_idx, surf_off, n_surf, c0 + lane);
+            tb = __double_as_longlong(__ldg(&con[c0 + lane].expiry));
+            rb = __double_as_longlong(__ldg(&con[c0 + lane].rate));
+        }
+        const long long pps = __shfl_up_sync(FULL, ps, 1), ptb = __shfl_up_sync(FULL, tb, 1),
+                        prb = __shfl_up_sync(FULL, rb, 1);
+        const unsigned starts = __ballot_sync(FULL, lane < cnt && (lane == 0 || ps != pps || tb != ptb || rb != prb));
+        for (int i = 0; i < cnt; ++i) {
+            const long long c = c0 + i;
+            const long long s = __shfl_sync(FULL, ps, i);
+            if ((starts >> i) & 1u) {
+                const unsigned later = i < 31 ? starts >> (i + 1) : 0u;
+                const int next = later ? i + __ffs((int)later) : cnt;
+                run_cache_discard(rc, lane);
+                rc.on = next - i >= 2 && rc.cap > 0;
+            }
+            if (!param_idx && n_surf > 1 && !ope_check(s >= 0 && s < n_surf, CHK_SURFACE)) continue;
+            run_unit<BATES, false, true>(c, which, con, params + s * stride, tol, out, integ, done, nbis_out, none,
+                                         0, smem_panels[warp], s_consts[warp], lane, R, &rc);
+        }
+    }
+}
+
+// Run probe of an automatic launch: counts the contracts that start a run
+// (the first of the call, of a surface, or a change of expiry or rate) and,
+// in its last block to finish, picks the contracts per unit: the largest
+// power of two up to 16 that is at most the mean run length and leaves every
+// warp of the run kernel's grid (run_warps) at least kRunsUnitsPerWarp units,
+// so that the queue's tail stays short.  Below kRunsMinPerUnit it keeps the
+// per-contract kernel.  It closes the work queue of the kernel that is not
+// to run (head[0]: the per-contract kernel's, head[16]: the run kernel's)
+// and leaves the choice in head[25] for the run kernel; head[24] holds its
+// two counters.  Both kernels are launched after it; the one whose queue is
+// closed ends after one atomic per warp.
+constexpr unsigned long long kQueueClosed = 1ull << 62;
+
+__global__ void __launch_bounds__(256) k_run_probe(const ope_contract* __restrict__ con, long long n,
+                                                   const int64_t* __restrict__ surf_off, long long n_surf,
+                                                   const int32_t* __restrict__ param_idx, unsigned long long* head,
+                                                   long long run_warps) {
+    __shared__ unsigned int part[8];
+    unsigned int* cnt = reinterpret_cast<unsigned int*>(head + 24);  // [0] starts, [1] blocks done
+    unsigned int mine = 0;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        bool start = c == 0;
+        if (!start) {
+            start = param_set(param_idx, surf_off, n_surf, c) != param_set(param_idx, surf_off, n_surf, c - 1) ||
+                    __double_as_longlong(__ldg(&con[c].expiry)) != __double_as_longlong(__ldg(&con[c - 1].expiry)) ||
+                    __double_as_longlong(__ldg(&con[c].rate)) != __double_as_longlong(__ldg(&con[c - 1].rate));
+        }
+        mine += start ? 1u : 0u;
+    }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, d);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = mine;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned int sum = 0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) sum += part[i];
+        atomicAdd(cnt, sum);
+        __threadfence();
+        if (atomicAdd(cnt + 1, 1u) == gridDim.x - 1) {
+            __threadfence();
+            const unsigned long long starts = atomicAdd(cnt, 0u);
+            int pu = kRunsMaxPerUnit;
+            while (pu >= kRunsMinPerUnit &&
+                   ((unsigned long long)n < (unsigned long long)pu * starts ||
+                    2ull * (unsigned long long)n < (unsigned long long)pu * kRunsUnitsPerWarp * (unsigned long long)run_warps))
+                pu >>= 1;
+            const bool runs = pu >= kRunsMinPerUnit;
+            head[25] = runs ? (unsigned long long)pu : 0ull;
+            __threadfence();
+            atomicExch(head + (runs ? 0 : 16), kQueueClosed);
+        }
     }
 }
 
@@ -303,6 +473,45 @@ int launch_impl(const ope_contract* con, size_t n, const int64_t* surf_offsets, 
     return OPE_OK;
 }
 
+// Grid of the run kernel (blocks of WARPS warps): the persistent grid,
+// capped by the warps the run cache holds and by the units of a launch of
+// per_unit contracts (the smallest the run probe may pick when automatic).
+template <bool BATES, int WARPS>
+int runs_grid(size_t n, const PriceScratch& s, int per_unit, double occupancy, int* grid) {
+    const int threads = WARPS * 32;
+    const size_t smem = WARPS * (sizeof(PanelStore) + kMaxPanels * sizeof(uint16_t));
+    OPE_TRY(persistent_grid(k_price_runs<BATES, WARPS>, threads, smem, occupancy, grid));
+    const int pu = per_unit > 0 ? per_unit : kRunsMinPerUnit;
+    const unsigned long long blocks = ((unsigned long long)n + pu - 1) / pu;
+    const unsigned long long need = (2ull * blocks + WARPS - 1) / WARPS;
+    const size_t cache_warps = s.runcache_bytes / kRunCacheWarpBytes;
+    *grid = (int)std::min<unsigned long long>({(unsigned long long)*grid, need, cache_warps / WARPS});
+    if (*grid < 1) return set_error(OPE_ERR_INVALID_ARG, "run cache too small for one block of warps");
+    return OPE_OK;
+}
+
+// per_unit 0: the run probe's choice (automatic launches).
+template <bool BATES, int WARPS>
+int launch_runs(const ope_contract* con, size_t n, const int64_t* surf_offsets, size_t n_surf,
+                const int32_t* param_idx, const double* params, double tol, double* out, const PriceScratch& s,
+                cudaStream_t st, int32_t* nbis_out, int per_unit, double occupancy) {
+    const int threads = WARPS * 32;
+    const size_t smem = WARPS * (sizeof(PanelStore) + kMaxPanels * sizeof(uint16_t));
+    int grid = 0;
+    OPE_TRY((runs_grid<BATES, WARPS>(n, s, per_unit, occupancy, &grid)));
+    const size_t cache_warps = s.runcache_bytes / kRunCacheWarpBytes;
+    RunCacheMem mem;
+    mem.cap = kRunCacheEntries;
+    mem.vals = static_cast<double*>(s.runcache);
+    mem.child = reinterpret_cast<uint32_t*>(static_cast<char*>(s.runcache) +
+                                            cache_warps * (size_t)kRunCacheEntries * 2 * 16 * sizeof(double));
+    k_price_runs<BATES, WARPS><<<grid, threads, smem, st>>>(con, (long long)n, surf_offsets, (long long)n_surf,
+                                                             param_idx, params, tol, out, s.integ, s.done,
+                                                             s.head + 16, nbis_out, per_unit, mem);
+    OPE_CHECK(cudaGetLastError());
+    return OPE_OK;
+}
+
 template <bool BATES>
 int launch_plain(int warps, const ope_contract* con, size_t n, const int64_t* surf_offsets, size_t n_surf,
                  const int32_t* param_idx, const double* params, double tol, double* out, const PriceScratch& s,
@@ -344,6 +553,12 @@ const uint64_t kTuneClassMax[kTuneClasses] = {1ull << 6,  1ull << 7,  1ull << 8,
                                                1ull << 12, 1ull << 13, 1ull << 14, 1ull << 15, 1ull << 16, 1ull << 17,
                                                1ull << 18, 1ull << 19, 1ull << 20, ~0ull};
 
+size_t run_cache_bytes() {
+    int sms = 0;
+    if (current_device_sms(&sms) != OPE_OK) return 0;
+    return (size_t)sms * kRunWarpsPerSm * kRunCacheWarpBytes;
+}
+
 int prepare_price_kernels() {
     int grid = 0;
     const int threads = 4 * 32;
@@ -364,6 +579,14 @@ int launch_price_persistent(int model, const ope_contract* con, size_t n, const 
     LaunchShape sh;
     if (!sink && !surf_mask) sh = shape ? *shape : price_shape(model, n);
     if (!s.order || n > 0xffffffffull) sh.deepest_first = 0;
+    // contracts per unit: fixed (2..32), automatic (0: probe for runs in
+    // calls of kRunsMinContracts or more), or one per unit; the run kernel
+    // needs the run cache and serves plain launches only
+    if (!s.runcache || sink || surf_mask || sh.per_unit < 0 || (sh.per_unit == 0 && n < kRunsMinContracts))
+        sh.per_unit = 1;
+    if (sh.per_unit > 32) sh.per_unit = 32;
+    const bool probe = sh.per_unit == 0;
+    if (sh.per_unit > 1) sh.deepest_first = 0;
     if (sh.warps != 1 && sh.warps != 2) sh.warps = 4;
     if (!(sh.occupancy > 0.0 && sh.occupancy <= 1.0)) sh.occupancy = 1.0;
     // completion counters, queue head and (for a deepest-first order) the
@@ -371,14 +594,19 @@ int launch_price_persistent(int model, const ope_contract* con, size_t n, const 
     const size_t done_bytes = align_up(n * sizeof(unsigned int), 256);
     const bool adjacent = reinterpret_cast<char*>(s.head) == reinterpret_cast<char*>(s.done) + done_bytes;
     const bool hist_adjacent = sh.deepest_first && reinterpret_cast<char*>(s.hist) == reinterpret_cast<char*>(s.head) + 256;
+    const size_t head_bytes = 256;  // both queue heads and the probe's words
     if (adjacent) {
-        OPE_CHECK(cudaMemsetAsync(s.done, 0, done_bytes + (hist_adjacent ? 256 + 512 : sizeof(unsigned long long)), st));
+        OPE_CHECK(cudaMemsetAsync(s.done, 0, done_bytes + (hist_adjacent ? 256 + 512 : head_bytes), st));
     } else {
         OPE_CHECK(cudaMemsetAsync(s.done, 0, n * sizeof(unsigned int), st));
-        OPE_CHECK(cudaMemsetAsync(s.head, 0, sizeof(unsigned long long), st));
+        OPE_CHECK(cudaMemsetAsync(s.head, 0, head_bytes, st));
     }
     if (sh.deepest_first && !(adjacent && hist_adjacent))
         OPE_CHECK(cudaMemsetAsync(s.hist, 0, 2 * kOrderBuckets * sizeof(unsigned int), st));
+    if (!sink && !surf_mask) {
+        tctx().last_per_unit = sh.per_unit;
+        tctx().last_probe = nullptr;
+    }
     const uint32_t* order = nullptr;
     if (sh.deepest_first) {
         OPE_TRY(build_order(model, con, n, surf_offsets, n_surf, param_idx, params, s, st));
@@ -393,6 +621,28 @@ int launch_price_persistent(int model, const ope_contract* con, size_t n, const 
         OPE_TRY((bates ? launch_impl<true, false, 4> : launch_impl<false, false, 4>)(
             con, n, surf_offsets, n_surf, param_idx, params, tol, out, s, st, nbis_out, surf_mask, none, nullptr,
             1.0));
+    } else if (sh.per_unit > 1) {
+        OPE_TRY((bates ? launch_runs<true, 4> : launch_runs<false, 4>)(con, n, surf_offsets, n_surf, param_idx, params,
+                                                                       tol, out, s, st, nbis_out, sh.per_unit,
+                                                                       sh.occupancy));
+    } else if (probe) {
+        // the probe closes one of the two queues; both kernels launch
+        tctx().last_probe = s.head + 25;
+        tctx().last_probe_stream = st;
+        int sms = 0;
+        OPE_TRY(current_device_sms(&sms));
+        const unsigned pb = (unsigned)std::max(1ll, std::min<long long>((long long)((n + 255) / 256), 4ll * sms));
+        int rgrid = 0;
+        OPE_TRY((bates ? runs_grid<true, 4> : runs_grid<false, 4>)(n, s, 0, sh.occupancy, &rgrid));
+        k_run_probe<<<pb, 256, 0, st>>>(con, (long long)n, surf_offsets, (long long)n_surf, param_idx, s.head,
+                                        4ll * rgrid);
+        OPE_CHECK(cudaGetLastError());
+        OPE_TRY((bates ? launch_plain<true> : launch_plain<false>)(sh.warps, con, n, surf_offsets, n_surf, param_idx,
+                                                                   params, tol, out, s, st, nbis_out, order,
+                                                                   sh.occupancy));
+        OPE_TRY((bates ? launch_runs<true, 4> : launch_runs<false, 4>)(con, n, surf_offsets, n_surf, param_idx, params,
+                                                                       tol, out, s, st, nbis_out, 0, sh.occupancy));
+        tctx().launches += 2;
     } else {
         OPE_TRY((bates ? launch_plain<true> : launch_plain<false>)(sh.warps, con, n, surf_offsets, n_surf, param_idx,
                                                                    params, tol, out, s, st, nbis_out, order,

@@ -116,6 +116,64 @@ __device__ __forceinline__ void gk_sums(double f, const LaneRule& R, double& Kl,
     Gr = __shfl_sync(FULL, v, 24);
 }
 
+// The run cache: node_cf's values at the panels that the contracts of one
+// run (consecutive contracts of one surface with the same expiry and rate,
+// integrating the same P1 or P2) have bisected, kept by the one warp that
+// integrates the run's contracts one after another.  Every panel of the
+// quadrature descends from [0, 1] by bisection and a bisection always
+// evaluates both children, so the cached panels form a binary tree: entry 0
+// is [0, 1], and each entry records the entries of its two children once
+// they have been evaluated.  Each live panel of the running integral carries
+// its entry (kNoEntry: not cached, nor are its descendants), so a bisection
+// finds its children's values with one load, without searching.  A contract
+// whose next panel is in the tree skips node_cf (the CF, its square root,
+// logarithm and exponentials) and pays only node_finish (its own phase and
+// one sin).  The tree lives in global memory (per warp: cap entries of 15
+// nodes x {w, a, u}); when it is full, further panels are evaluated
+// uncached.  The cached values are the ones node_cf returns (u is
+// recomputed from the node, bit for bit), so a contract's price is
+// bit-identical with and without the cache.  An entry's w and a are one
+// 128-byte line each (15 nodes and a zero pad, written whole so that L2
+// never fetches the rest of a partly written line from DRAM).
+constexpr uint16_t kNoEntry = 0xffff;
+constexpr uint32_t kNoChildren = 0xffffffffu;
+
+struct RunCacheWarp {
+    double* w;          // [cap][16]
+    double* a;          // [cap][16]
+    uint32_t* child;    // [cap]: children's entries, left | right << 16 (kNoChildren: none yet)
+    uint16_t* slot;     // shared, [kMaxPanels]: entry of each live panel of the running integral
+    int cap;            // entries (<= 65535)
+    int n_alloc;        // entries in use (warp-uniform; 0 at the start of a run)
+    bool on;            // cache this integral's panels (warp-uniform)
+};
+
+// node_cf as a real call, for the cached loop: a cache hit needs few
+// registers, and the call keeps the node evaluation's register demand (and
+// its spills) out of the hit path.
+// (Internal linkage, so that ptxas allocates its registers within the
+// calling kernel's budget.)
+namespace {
+template <bool BATES>
+__device__ __noinline__ NodeCf node_cf_call(const CfConsts& C, double tn) {
+    return node_cf<BATES>(C, tn);
+}
+}  // namespace
+
+// End of a run: its entries will be rewritten before they are read again, so
+// their lines are dropped from L2 without being written back to DRAM
+// (discard.global.L2), which keeps the dead data of finished runs from
+// costing DRAM bandwidth.  Warp-collective.
+__device__ __forceinline__ void run_cache_discard(RunCacheWarp& rc, int lane) {
+    __syncwarp();
+    for (int j = lane; j < 2 * rc.n_alloc; j += 32) {
+        const double* line = j < rc.n_alloc ? rc.w + (size_t)j * 16 : rc.a + (size_t)(j - rc.n_alloc) * 16;
+        asm volatile("discard.global.L2 [%0], 128;" ::"l"(line) : "memory");
+    }
+    __syncwarp();
+    rc.n_alloc = 0;
+}
+
 // Step hooks of gk_integrate_warp.  The pricing kernels use NoTrace (empty
 // and inlined: no code); the QAG trace kernel (trace.cu) records every step.
 //   first(lane, f, k0, e0): the first panel [0, 1] (f: this lane's integrand
@@ -134,9 +192,15 @@ struct NoTrace {
 // live-panel list (nbis + 1 entries) is left in L.  The first panel and every
 // bisection go through ONE call site of the integrand, so the (large) inlined
 // node evaluation exists once in the instruction stream.
-template <bool BATES, class Trace = NoTrace>
+//
+// CACHED: with the run cache `rc` (which may be off for this integral): each
+// step first looks its panel(s) up in the tree (a hit: both children, or the
+// root, already evaluated) and otherwise evaluates node_cf and, while the
+// tree has room and the bisected panel is in it, stores the children.
+template <bool BATES, bool CACHED = false, class Trace = NoTrace>
 __device__ __forceinline__ double gk_integrate_warp(const CfConsts& C, double tol, PanelStore& L, int lane,
-                                                    const LaneRule& R, int* nbis, const Trace& tr = Trace()) {
+                                                    const LaneRule& R, int* nbis, const Trace& tr = Trace(),
+                                                    RunCacheWarp* rc = nullptr) {
     const unsigned FULL = 0xffffffffu;
     double total = 0.0, err = 0.0;
     int len = 0;
@@ -145,9 +209,43 @@ __device__ __forceinline__ double gk_integrate_warp(const CfConsts& C, double to
     bool active = (R.half == 0) && R.node;
     double aw = 0.0, bw = 1.0, m = 0.5, kw = 0.0, ew = 0.0;
     int w = 0;
+    // cache mode of the step (warp-uniform): hit = read entries el_/er_,
+    // put = evaluate and store into them; neither = evaluate uncached.  The
+    // first step's panel [0, 1] is entry 0 (read as the left child).
+    bool hit = false, put = false;
+    int el_ = kNoEntry, er_ = kNoEntry, sw_ = kNoEntry;  // sw_: entry of the bisected panel
+    if (CACHED && rc->on) {
+        if (rc->n_alloc > 0) {
+            hit = true;
+            el_ = 0;
+        } else if (rc->cap > 0) {
+            put = true;
+            el_ = 0;
+            rc->n_alloc = 1;
+        }
+    }
     while (true) {
         const double c = 0.5 * (pa + pb), h = 0.5 * (pb - pa);
-        const double f = active ? node_value<BATES>(C, __dadd_rn(c, __dmul_rn(h, R.x))) : 0.0;
+        NodeCf nc{0.0, 0.0, 0.0};
+        if (CACHED && hit) {
+            if (active) {
+                const size_t i = (size_t)(R.half ? er_ : el_) * 16 + (lane & 15);
+                nc = NodeCf{__ldcg(rc->w + i), __ldcg(rc->a + i), node_u_of(__dadd_rn(c, __dmul_rn(h, R.x)))};
+            }
+        } else {
+            if (active) {
+                const double tn = __dadd_rn(c, __dmul_rn(h, R.x));
+                nc = CACHED ? node_cf_call<BATES>(C, tn) : node_cf<BATES>(C, tn);
+            }
+            // the half-warps that evaluated a child write its entry, the
+            // pad lane (15 or 31) the 16th element
+            if (CACHED && put && (active || (!R.node && (len > 0 || R.half == 0)))) {
+                const size_t i = (size_t)(R.half ? er_ : el_) * 16 + (lane & 15);
+                __stcg(rc->w + i, active ? nc.w : 0.0);
+                __stcg(rc->a + i, active ? nc.a : 0.0);
+            }
+        }
+        const double f = active ? node_finish(C.x, nc) : 0.0;
         double Kl, Gl, Kr, Gr;
         gk_sums(f, R, Kl, Gl, Kr, Gr);
         if (len == 0) {
@@ -162,6 +260,10 @@ __device__ __forceinline__ double gk_integrate_warp(const CfConsts& C, double to
             err = e0;
             len = 1;
             tr.first(lane, f, k0, e0);
+            if (CACHED && rc->on && lane == 0) {
+                rc->slot[0] = (uint16_t)el_;
+                if (put) rc->child[0] = kNoChildren;
+            }
         } else {
             const double hl = 0.5 * (m - aw), hr = 0.5 * (bw - m);
             const double kl = __dmul_rn(Kl, hl), el = __dmul_rn(fabs(Kl - Gl), hl);
@@ -185,6 +287,20 @@ __device__ __forceinline__ double gk_integrate_warp(const CfConsts& C, double to
                 L.k[len] = kr;
                 L.a[len] = m;
                 L.b[len] = bw;
+                if (CACHED && rc->on) {
+                    if (w != last) rc->slot[w] = rc->slot[last];
+                    rc->slot[last] = (uint16_t)el_;
+                    rc->slot[len] = (uint16_t)er_;
+                    if (put) {
+                        rc->child[el_] = kNoChildren;
+                        rc->child[er_] = kNoChildren;
+                        rc->child[sw_] = (uint32_t)el_ | ((uint32_t)er_ << 16);
+                    } else if (hit) {
+                        // the children's own child words, read when they are bisected
+                        asm volatile("prefetch.global.L1 [%0];" ::"l"(rc->child + el_));
+                        asm volatile("prefetch.global.L1 [%0];" ::"l"(rc->child + er_));
+                    }
+                }
             }
             ++len;
         }
@@ -224,6 +340,26 @@ __device__ __forceinline__ double gk_integrate_warp(const CfConsts& C, double to
         pa = R.half ? m : aw;
         pb = R.half ? bw : m;
         active = R.node;
+        if (CACHED && rc->on) {
+            // the children of panel w: in the tree (hit), or new entries (put)
+            // while the tree has room for both and w is in it
+            sw_ = rc->slot[w];
+            hit = put = false;
+            el_ = er_ = kNoEntry;
+            if (sw_ != kNoEntry) {
+                const uint32_t ch = rc->child[sw_];
+                if (ch != kNoChildren) {
+                    hit = true;
+                    el_ = (int)(ch & 0xffffu);
+                    er_ = (int)(ch >> 16);
+                } else if (rc->n_alloc + 2 <= rc->cap) {
+                    put = true;
+                    el_ = rc->n_alloc;
+                    er_ = rc->n_alloc + 1;
+                    rc->n_alloc += 2;
+                }
+            }
+        }
         __syncwarp();  // every lane has read entry w before lane 0 rewrites it
     }
     *nbis = len - 1;

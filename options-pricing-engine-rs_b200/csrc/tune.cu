@@ -122,6 +122,8 @@ ope_tune_entry default_entry(int cls) {
     e.shape.warps_per_block = 4;
     e.shape.deepest_first = 0;
     e.shape.occupancy = 1.0;
+    e.shape.per_unit = 0;
+    e.shape.reserved = 0;
     e.ms_default = 0.0;
     e.ms_tuned = 0.0;
     return e;
@@ -171,6 +173,7 @@ LaunchShape price_shape(int model, size_t n) {
     sh.warps = e.shape.warps_per_block;
     sh.deepest_first = e.shape.deepest_first;
     sh.occupancy = e.shape.occupancy;
+    sh.per_unit = e.shape.per_unit;
     return sh;
 }
 
@@ -259,6 +262,7 @@ int ope_autotune(int32_t model, uint32_t flags, ope_tune_entry* out_entries) {
                 e.shape.warps_per_block = best.warps;
                 e.shape.deepest_first = best.deepest_first;
                 e.shape.occupancy = best.occupancy;
+                e.shape.per_unit = best.per_unit;
                 e.ms_tuned = t_best;
             } else {
                 e.ms_tuned = t_def;
@@ -298,6 +302,7 @@ int ope_set_tune_table(int32_t model, const ope_tune_entry* entries) {
             return set_error(OPE_ERR_INVALID_ARG, "deepest_first must be 0 or 1");
         if (!(sh.occupancy > 0.0 && sh.occupancy <= 1.0))
             return set_error(OPE_ERR_INVALID_ARG, "occupancy must be in (0, 1]");
+        if (sh.per_unit < 0 || sh.per_unit > 32) return set_error(OPE_ERR_INVALID_ARG, "per_unit must be in 0..32");
     }
     OPE_TRY(ensure_device());
     const int m = model == OPE_MODEL_BATES ? 1 : 0;
@@ -308,6 +313,20 @@ int ope_set_tune_table(int32_t model, const ope_tune_entry* entries) {
         T.e[m][i].max_contracts = kTuneClassMax[i];
     }
     T.tuned[m] = true;
+    return OPE_OK;
+}
+
+int ope_last_per_unit(int32_t* out_per_unit) {
+    if (!out_per_unit) return set_error(OPE_ERR_INVALID_ARG, "NULL argument");
+    ThreadCtx& c = tctx();
+    if (!c.last_probe) {
+        *out_per_unit = c.last_per_unit;
+        return OPE_OK;
+    }
+    unsigned long long v = 0;
+    OPE_CHECK(cudaStreamSynchronize(c.last_probe_stream));
+    OPE_CHECK(cudaMemcpy(&v, c.last_probe, sizeof(v), cudaMemcpyDeviceToHost));
+    *out_per_unit = v ? (int32_t)v : 1;
     return OPE_OK;
 }
 

@@ -105,7 +105,8 @@ _sig("ope_measure_fp64_peak", ctypes.c_int, [ctypes.POINTER(_d), ctypes.POINTER(
 _sig("ope_trace_integral", ctypes.c_int, [_i32, _vp, _vp, _i32, _d, _vp, _i32, ctypes.POINTER(_i32), ctypes.POINTER(_d)])
 
 class LaunchShape(ctypes.Structure):
-    _fields_ = [("warps_per_block", ctypes.c_int32), ("deepest_first", ctypes.c_int32), ("occupancy", ctypes.c_double)]
+    _fields_ = [("warps_per_block", ctypes.c_int32), ("deepest_first", ctypes.c_int32), ("occupancy", ctypes.c_double),
+                ("per_unit", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 class TuneEntry(ctypes.Structure):
@@ -118,6 +119,7 @@ TUNE_QUICK = 1    # OPE_TUNE_QUICK
 _sig("ope_autotune", ctypes.c_int, [_i32, ctypes.c_uint32, ctypes.POINTER(TuneEntry)])
 _sig("ope_set_autotune", ctypes.c_int, [_i32])
 _sig("ope_get_tune_table", ctypes.c_int, [_i32, ctypes.POINTER(TuneEntry), ctypes.POINTER(_i32)])
+_sig("ope_last_per_unit", ctypes.c_int, [ctypes.POINTER(_i32)])
 _sig("ope_set_tune_table", ctypes.c_int, [_i32, ctypes.POINTER(TuneEntry)])
 
 _lib = None

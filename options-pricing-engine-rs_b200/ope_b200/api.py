@@ -495,7 +495,8 @@ def measure_fp64_peak() -> tuple[float, float]:
 def _tune_rows(entries) -> list[dict]:
     return [{"max_contracts": int(e.max_contracts) if e.max_contracts < 2 ** 63 else None,
              "warps_per_block": int(e.shape.warps_per_block), "deepest_first": bool(e.shape.deepest_first),
-             "occupancy": float(e.shape.occupancy), "ms_default": float(e.ms_default), "ms_tuned": float(e.ms_tuned)}
+             "occupancy": float(e.shape.occupancy), "per_unit": int(e.shape.per_unit),
+             "ms_default": float(e.ms_default), "ms_tuned": float(e.ms_tuned)}
             for e in entries]
 
 
@@ -522,9 +523,18 @@ def set_tune_table(model: int, rows: list[dict]) -> None:
         e.shape.warps_per_block = int(r["warps_per_block"])
         e.shape.deepest_first = int(bool(r["deepest_first"]))
         e.shape.occupancy = float(r["occupancy"])
+        e.shape.per_unit = int(r.get("per_unit", 0))
         e.ms_default = float(r.get("ms_default", 0.0))
         e.ms_tuned = float(r.get("ms_tuned", 0.0))
     check(load().ope_set_tune_table(model, entries))
+
+
+def last_per_unit() -> int:
+    """Contracts per unit of this thread's last plain pricing launch (1: one
+    per unit; automatic launches report the run probe's choice)."""
+    v = ctypes.c_int32()
+    check(load().ope_last_per_unit(ctypes.byref(v)))
+    return int(v.value)
 
 
 def tune_table(model: int) -> tuple[list[dict], bool]:
@@ -626,5 +636,5 @@ __all__ = [
     "calibrate_global", "calibrate_heston_regularized", "calibrate_bates_regularized", "calibrate_heston_multistart",
     "calibrate_bates_multistart", "calibrate_heston_global", "calibrate_bates_global",
     "calibrate_heston_global_regularized", "calibrate_bates_global_regularized", "trace_integral",
-    "autotune", "set_autotune", "tune_table", "set_tune_table",
+    "autotune", "set_autotune", "tune_table", "set_tune_table", "last_per_unit",
 ]

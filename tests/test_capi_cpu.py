@@ -34,6 +34,33 @@ def test_record_layouts_match_header():
     assert list(CONTRACT_DTYPE.names) == ["spot", "strike", "expiry", "rate", "div_yield", "vol", "opt_type", "pad"]
 
 
+def test_tune_structs_match_header(tmp_path):
+    """ope_launch_shape / ope_tune_entry: the ctypes mirrors have the header's
+    sizes and field offsets (compiled with the host C compiler)."""
+    import ctypes
+    import subprocess
+
+    from ope_b200 import _lib
+
+    fields = {"ope_launch_shape": ["warps_per_block", "deepest_first", "occupancy", "per_unit", "reserved"],
+              "ope_tune_entry": ["max_contracts", "shape", "ms_default", "ms_tuned"]}
+    src = ['#include <stdio.h>', '#include <stddef.h>', '#include "ope.h"', "int main(void) {"]
+    for st, fs in fields.items():
+        src.append(f'printf("%zu\\n", sizeof({st}));')
+        src += [f'printf("%zu\\n", offsetof({st}, {f}));' for f in fs]
+    src.append("return 0; }")
+    c = tmp_path / "layout.c"
+    c.write_text("\n".join(src))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(c), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    want = []
+    for mirror, fs in ((_lib.LaunchShape, fields["ope_launch_shape"]), (_lib.TuneEntry, fields["ope_tune_entry"])):
+        want.append(ctypes.sizeof(mirror))
+        want += [getattr(mirror, f).offset for f in fs]
+    assert got == want
+
+
 @pytest.mark.gpu
 def test_library_runs_on_sm100a(ope):
     """The library carries sm_100a code only: on the device it reports compute
