@@ -70,6 +70,7 @@ def parse_args():
     ap.add_argument("--serving-rates", default="100,1000,5000,10000,15000,20000")
     ap.add_argument("--serving-seconds", type=float, default=10.0, help="seconds of arrivals per serving rate")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shape (no ope_autotune)")
+    ap.add_argument("--no-grid", action="store_true", help="skip the grid-surface (config-2 layout) section")
     return ap.parse_args()
 
 
@@ -504,6 +505,68 @@ def bench_implied_vol(args, w, dev, flush, stream, d_con, d_prices, prices) -> d
     return out
 
 
+def bench_grid_surfaces(args, dev, flush, stream) -> dict:
+    """Surfaces laid out expiry by expiry (the uneven strike x expiry grids of
+    config 2, 4096 surfaces, ~1.46M contracts; Heston, and the same grids with
+    Bates parameters): the strikes of one expiry share the characteristic
+    function per panel in the run kernel.  Kernel time of the automatic launch
+    (a device probe picks the run kernel and its contracts per unit) against
+    one contract per unit, bit-identity of the two, and the oracle on a
+    sample."""
+    import torch
+
+    import ope_b200 as ope
+    from ope_b200 import workloads as W
+    from oracle import oracle as O
+
+    saved = {m: ope.tune_table(m)[0] for m in (ope.MODEL_HESTON, ope.MODEL_BATES)}
+    base = W.c2()
+    rng = np.random.default_rng(9)
+    ns = base.params.shape[0]
+    bates_params = np.concatenate([base.params, rng.uniform(0, 1.5, (ns, 1)), rng.uniform(-0.3, 0.1, (ns, 1)),
+                                   rng.uniform(0.05, 0.4, (ns, 1))], axis=1)
+    out = {"what": "config-2 grids (expiry-major): automatic launch (run probe -> run kernel) vs one contract per "
+                   "unit, device buffers, L2 flushed between steps", "unit": UNIT}
+    try:
+        for name, model, params in (("heston", ope.MODEL_HESTON, base.params), ("bates", ope.MODEL_BATES, bates_params)):
+            d_con = torch.from_numpy(base.contracts.view(np.uint8).copy()).to(dev)
+            d_off = torch.from_numpy(base.surf_offsets.copy()).to(dev)
+            d_par = torch.from_numpy(np.ascontiguousarray(params)).to(dev)
+            res, prices = {}, {}
+            for mode, pu in (("automatic", 0), ("one_contract_per_unit", 1)):
+                rows = [dict(r, per_unit=pu) for r in saved[model]]
+                ope.set_tune_table(model, rows)
+                d_out = torch.full((base.n,), float("nan"), dtype=torch.float64, device=dev)
+                ms = []
+                for i in range(args.warmup + args.steps):
+                    flush.zero_()
+                    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    a.record(stream)
+                    ope.price_surfaces_device(model, d_con, base.n, d_off, base.n_surf, d_par, d_out, tol=base.tol,
+                                              stream=stream.cuda_stream)
+                    b.record(stream)
+                    torch.cuda.synchronize()
+                    if i >= args.warmup:
+                        ms.append(a.elapsed_time(b))
+                per_unit = ope.last_per_unit()
+                prices[mode] = d_out.cpu().numpy()
+                res[mode] = {"kernel_ms": float(np.mean(ms)), "value": base.n / (np.mean(ms) * 1e-3),
+                             "contracts_per_unit": per_unit}
+            res["speedup"] = res["one_contract_per_unit"]["kernel_ms"] / res["automatic"]["kernel_ms"]
+            res["bit_identical"] = bool(np.array_equal(prices["automatic"].view(np.int64),
+                                                       prices["one_contract_per_unit"].view(np.int64)))
+            pick = np.sort(np.random.default_rng(3).choice(base.n, 400, replace=False))
+            orc = O.batch_price(base.contracts[pick], params, model == ope.MODEL_BATES, base.tol,
+                                surf_idx=base.surf_idx()[pick])
+            res["max_abs_err_over_spot"] = float(np.max(np.abs(prices["automatic"][pick] - orc)) / 100.0)
+            res["n_contracts"] = int(base.n)
+            out[name] = res
+    finally:
+        for m, rows in saved.items():
+            ope.set_tune_table(m, rows)
+    return out
+
+
 def bench_serving(args, tuned: bool) -> dict:
     """Config 5: Poisson arrivals, 80 % Bates surface reprices / 20 % Heston
     calibrations, sizes log-uniform in [20, 2000] contracts.  For every offered
@@ -783,6 +846,8 @@ def run_ours(args) -> None:
         line["greeks"] = bench_greeks(args, w, dev, flush, stream)
     if rank == 0 and world == 1 and not args.no_gradient:
         line["implied_vol"] = bench_implied_vol(args, w, dev, flush, stream, d_con, d_out, ref_prices)
+    if rank == 0 and world == 1 and not args.no_grid:
+        line["grid_surfaces"] = bench_grid_surfaces(args, dev, flush, stream)
     if rank == 0 and world == 1 and not args.no_calib:
         line["calibration"] = bench_calibration(args)
     if rank == 0 and world == 1 and not args.no_serving:

@@ -331,50 +331,78 @@ __global__ void __launch_bounds__(WARPS * 32, OPE_RUNS_MINB * 4 / WARPS)
     }
 }
 
-// Run probe of an automatic launch: counts the contracts that start a run
-// (the first of the call, of a surface, or a change of expiry or rate) and,
-// in its last block to finish, picks the contracts per unit: the largest
-// power of two up to 16 that is at most the mean run length and leaves every
-// warp of the run kernel's grid (run_warps) at least kRunsUnitsPerWarp units,
-// so that the queue's tail stays short.  Below kRunsMinPerUnit it keeps the
-// per-contract kernel.  It closes the work queue of the kernel that is not
-// to run (head[0]: the per-contract kernel's, head[16]: the run kernel's)
-// and leaves the choice in head[25] for the run kernel; head[24] holds its
-// two counters.  Both kernels are launched after it; the one whose queue is
-// closed ends after one atomic per warp.
+// Run probe of an automatic launch: counts, on a sample of the call, the
+// contracts that start a run (the first of a surface, or a change of
+// expiry or rate) and, in its last block to finish, picks the contracts per
+// unit: the largest power of two up to 16 that is at most the sample's mean
+// run length and leaves every warp of the run kernel's grid (run_warps) at
+// least kRunsUnitsPerWarp units, so that the queue's tail stays short.
+// Below kRunsMinPerUnit it keeps the per-contract kernel.  The sample: up to
+// kProbeChunks chunks of 32 consecutive contracts spread evenly over the
+// call, one warp each, every lane reading one contract's expiry and rate
+// (the predecessor's come by shuffle; contracts in pinned host memory are
+// read over PCIe, so the probe reads as little as it can).  It closes the
+// work queue of the kernel that is not to run (head[0]: the per-contract
+// kernel's, head[16]: the run kernel's) and leaves the choice in head[25]
+// for the run kernel; head[26..27] hold its counters.  Both kernels are
+// launched after it; the one whose queue is closed ends after one atomic
+// per warp.  The choice only moves time: prices are the same either way.
 constexpr unsigned long long kQueueClosed = 1ull << 62;
+constexpr long long kProbeChunks = 2048;
 
 __global__ void __launch_bounds__(256) k_run_probe(const ope_contract* __restrict__ con, long long n,
                                                    const int64_t* __restrict__ surf_off, long long n_surf,
                                                    const int32_t* __restrict__ param_idx, unsigned long long* head,
                                                    long long run_warps) {
-    __shared__ unsigned int part[8];
-    unsigned int* cnt = reinterpret_cast<unsigned int*>(head + 24);  // [0] starts, [1] blocks done
-    unsigned int mine = 0;
-    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
-        bool start = c == 0;
-        if (!start) {
-            start = param_set(param_idx, surf_off, n_surf, c) != param_set(param_idx, surf_off, n_surf, c - 1) ||
-                    __double_as_longlong(__ldg(&con[c].expiry)) != __double_as_longlong(__ldg(&con[c - 1].expiry)) ||
-                    __double_as_longlong(__ldg(&con[c].rate)) != __double_as_longlong(__ldg(&con[c - 1].rate));
+    __shared__ unsigned int part[2][8];
+    const unsigned FULL = 0xffffffffu;
+    unsigned int* cnt = reinterpret_cast<unsigned int*>(head + 26);  // [0] starts, [1] sampled, [2] blocks done
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const long long chunks = (n + 31) / 32;
+    const long long samples = chunks < kProbeChunks ? chunks : kProbeChunks;
+    unsigned int starts = 0, seen = 0;
+    for (long long k = (long long)blockIdx.x * (blockDim.x >> 5) + wib; k < samples;
+         k += (long long)gridDim.x * (blockDim.x >> 5)) {
+        const long long c0 = (k * chunks / samples) * 32;
+        const long long c = c0 + lane;
+        const bool in = c < n;
+        long long ps = -1, tb = 0, rb = 0;
+        if (in) {
+            ps = param_set(param_idx, surf_off, n_surf, c);
+            tb = __double_as_longlong(__ldg(&con[c].expiry));
+            rb = __double_as_longlong(__ldg(&con[c].rate));
         }
-        mine += start ? 1u : 0u;
+        long long pps = __shfl_up_sync(FULL, ps, 1), ptb = __shfl_up_sync(FULL, tb, 1), prb = __shfl_up_sync(FULL, rb, 1);
+        bool start = true;
+        if (lane == 0 && c0 > 0) {
+            pps = param_set(param_idx, surf_off, n_surf, c0 - 1);
+            ptb = __double_as_longlong(__ldg(&con[c0 - 1].expiry));
+            prb = __double_as_longlong(__ldg(&con[c0 - 1].rate));
+        }
+        if (c > 0) start = ps != pps || tb != ptb || rb != prb;
+        starts += __popc(__ballot_sync(FULL, in && start));
+        seen += __popc(__ballot_sync(FULL, in));
     }
-#pragma unroll
-    for (int d = 16; d > 0; d >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, d);
-    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = mine;
+    if (lane == 0) {
+        part[0][wib] = starts;
+        part[1][wib] = seen;
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
-        unsigned int sum = 0;
-        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) sum += part[i];
-        atomicAdd(cnt, sum);
+        unsigned int st = 0, se = 0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) {
+            st += part[0][i];
+            se += part[1][i];
+        }
+        atomicAdd(cnt, st);
+        atomicAdd(cnt + 1, se);
         __threadfence();
-        if (atomicAdd(cnt + 1, 1u) == gridDim.x - 1) {
+        if (atomicAdd(cnt + 2, 1u) == gridDim.x - 1) {
             __threadfence();
-            const unsigned long long starts = atomicAdd(cnt, 0u);
+            const unsigned long long s_starts = atomicAdd(cnt, 0u), s_seen = atomicAdd(cnt + 1, 0u);
             int pu = kRunsMaxPerUnit;
             while (pu >= kRunsMinPerUnit &&
-                   ((unsigned long long)n < (unsigned long long)pu * starts ||
+                   (s_seen < (unsigned long long)pu * s_starts ||
                     2ull * (unsigned long long)n < (unsigned long long)pu * kRunsUnitsPerWarp * (unsigned long long)run_warps))
                 pu >>= 1;
             const bool runs = pu >= kRunsMinPerUnit;
@@ -631,7 +659,8 @@ int launch_price_persistent(int model, const ope_contract* con, size_t n, const 
         tctx().last_probe_stream = st;
         int sms = 0;
         OPE_TRY(current_device_sms(&sms));
-        const unsigned pb = (unsigned)std::max(1ll, std::min<long long>((long long)((n + 255) / 256), 4ll * sms));
+        const long long probe_warps = std::min<long long>((long long)((n + 31) / 32), kProbeChunks);
+        const unsigned pb = (unsigned)std::max(1ll, std::min<long long>((probe_warps + 7) / 8, 2ll * sms));
         int rgrid = 0;
         OPE_TRY((bates ? runs_grid<true, 4> : runs_grid<false, 4>)(n, s, 0, sh.occupancy, &rgrid));
         k_run_probe<<<pb, 256, 0, st>>>(con, (long long)n, surf_offsets, (long long)n_surf, param_idx, s.head,
