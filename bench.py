@@ -71,6 +71,8 @@ def parse_args():
     ap.add_argument("--serving-seconds", type=float, default=10.0, help="seconds of arrivals per serving rate")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shape (no ope_autotune)")
     ap.add_argument("--no-grid", action="store_true", help="skip the grid-surface (config-2 layout) section")
+    ap.add_argument("--grid-only", action="store_true",
+                    help="run only the grid-surface section (1 GPU) and print its JSON object")
     return ap.parse_args()
 
 
@@ -892,6 +894,12 @@ def main():
         sys.exit(rc)
     if args.impl == "reference":
         run_reference(args)
+    elif args.grid_only:
+        import torch
+
+        dev = torch.device("cuda", 0)
+        flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
+        print(json.dumps(bench_grid_surfaces(args, dev, flush, torch.cuda.current_stream())), flush=True)
     else:
         run_ours(args)
 
