@@ -313,14 +313,14 @@ int batch_price(int32_t model, const ope_contract* contracts, size_t n, const vo
     const int stride = param_stride(model);
     if (device_ptrs(opts)) {
         void* ws;
-        const size_t b_run = price_run_bytes(model, n);
+        const size_t b_run = price_run_bytes(model, n, price_scratch_bytes(n));
         OPE_TRY(ensure_workspace(price_scratch_bytes(n) + b_run, &ws, user_stream(opts)));
         return launch_price_persistent(model, contracts, n, nullptr, 1, nullptr, static_cast<const double*>(params),
                                        tol, out, carve_price_scratch(ws, n, b_run), user_stream(opts));
     }
     ThreadCtx& c = tctx();
-    const size_t b_con = align_up(n * sizeof(ope_contract), 256), b_par = 256, b_out = align_up(n * sizeof(double), 256),
-                 b_run = price_run_bytes(model, n);
+    const size_t b_con = align_up(n * sizeof(ope_contract), 256), b_par = 256, b_out = align_up(n * sizeof(double), 256);
+    const size_t b_run = price_run_bytes(model, n, b_con + b_par + b_out + price_scratch_bytes(n));
     void* ws;
     OPE_TRY(ensure_workspace(b_con + b_par + b_out + price_scratch_bytes(n) + b_run, &ws, c.stream));
     char* p = static_cast<char*>(ws);
@@ -725,7 +725,7 @@ int ope_price_surfaces_stats(int32_t model, const ope_contract* contracts, size_
     const int stride = param_stride(model);
     if (device_ptrs(opts)) {
         void* ws;
-        const size_t b_run = price_run_bytes(model, n);
+        const size_t b_run = price_run_bytes(model, n, price_scratch_bytes(n));
         OPE_TRY(ensure_workspace(price_scratch_bytes(n) + b_run, &ws, user_stream(opts)));
         return launch_price_persistent(model, contracts, n, surf_offsets, n_surf, nullptr,
                                        static_cast<const double*>(params), tol, out_prices,
@@ -738,7 +738,8 @@ int ope_price_surfaces_stats(int32_t model, const ope_contract* contracts, size_
     ThreadCtx& c = tctx();
     const size_t b_con = align_up(n * sizeof(ope_contract), 256), b_off = align_up((n_surf + 3) * sizeof(int64_t), 256),
                  b_par = align_up(n_surf * stride * sizeof(double), 256), b_out = align_up(n * sizeof(double), 256),
-                 b_nb = out_bisections ? align_up(2 * n * sizeof(int32_t), 256) : 0, b_run = price_run_bytes(model, n);
+                 b_nb = out_bisections ? align_up(2 * n * sizeof(int32_t), 256) : 0;
+    const size_t b_run = price_run_bytes(model, n, b_con + b_off + b_par + b_out + b_nb + price_scratch_bytes(n));
     void* ws;
     OPE_TRY(ensure_workspace(b_con + b_off + b_par + b_out + b_nb + price_scratch_bytes(n) + b_run, &ws, c.stream));
     char* p = static_cast<char*>(ws);

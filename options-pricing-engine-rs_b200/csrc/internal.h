@@ -127,11 +127,13 @@ struct PriceScratch {
 size_t price_scratch_bytes(size_t n);
 PriceScratch carve_price_scratch(void* base, size_t n);
 // The same with the run cache (run_bytes of it, 0: none) right after the
-// price_scratch_bytes(n) bytes; price_run_bytes(model, n): the run cache a
-// plain launch of n contracts wants under the current launch shape (0 or
-// run_cache_bytes()).  Callers size and carve with one value of it.
+// price_scratch_bytes(n) bytes; price_run_bytes(model, n, other_bytes): the
+// run cache a plain launch of n contracts wants under the current launch
+// shape (0 or run_cache_bytes(); 0 too when it would take a workspace of
+// other_bytes past the thread's limit).  Callers size and carve with one
+// value of it.
 PriceScratch carve_price_scratch(void* base, size_t n, size_t run_bytes);
-size_t price_run_bytes(int model, size_t n);
+size_t price_run_bytes(int model, size_t n, size_t other_bytes);
 
 // Launch shape of a plain pricing launch: warps per block (each warp one
 // integral, so warps / 2 contracts per block) of the persistent grid, whether

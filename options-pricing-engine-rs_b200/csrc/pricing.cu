@@ -81,9 +81,14 @@ PriceScratch carve_price_scratch(void* base, size_t n, size_t run_bytes) {
     return s;
 }
 
-size_t price_run_bytes(int model, size_t n) {
+size_t price_run_bytes(int model, size_t n, size_t other_bytes) {
     const int pu = price_shape(model, n).per_unit;
-    return (pu > 1 || (pu == 0 && n >= kRunsMinContracts)) ? run_cache_bytes() : 0;
+    if (!(pu > 1 || (pu == 0 && n >= kRunsMinContracts))) return 0;
+    const size_t b = run_cache_bytes();
+    // under a workspace limit the run cache is optional: without it the call
+    // takes one contract per unit, with the same prices
+    const size_t limit = tctx().ws_limit;
+    return (limit && other_bytes + b > limit) ? 0 : b;
 }
 
 PanelSink carve_panel_sink(void* base, size_t n, int n_slots, const int32_t* slot) {

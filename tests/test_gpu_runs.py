@@ -192,3 +192,20 @@ def test_tune_table_rejects_bad_per_unit(ope):
     bad = [dict(r, per_unit=33) for r in rows]
     with pytest.raises(Exception, match="per_unit"):
         ope.set_tune_table(ope.MODEL_HESTON, bad)
+
+
+def test_workspace_limit_drops_the_run_cache_not_the_call(ope, per_unit):
+    """Under a workspace limit too small for the run cache (~157 MB) but large
+    enough for the call itself, an automatic grid call still prices: it takes
+    one contract per unit, with the same bits as the run kernel."""
+    con, off, params = _grid(900, seed=26)
+    per_unit(ope.MODEL_HESTON, 0)
+    ref = _prices(ope, ope.MODEL_HESTON, con, off, params)
+    assert ope.last_per_unit() >= 4
+    try:
+        ope.set_workspace_limit(96 << 20)
+        got = _prices(ope, ope.MODEL_HESTON, con, off, params)
+        assert ope.last_per_unit() == 1
+    finally:
+        ope.set_workspace_limit(0)
+    assert np.array_equal(got.view(np.int64), ref.view(np.int64))
