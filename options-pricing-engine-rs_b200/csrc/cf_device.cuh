@@ -25,8 +25,8 @@
 // Of Z only the phase u x depends on the strike (x = ln(S/K)); the rest is a
 // function of the node, the expiry, the rate, the parameters and the
 // integral.  So the evaluation is split: node_cf gives the strike-free part
-// (W = e^{Re Z}/((1-t)t), Im Z without u x, and u), node_finish adds one
-// strike's phase and forms the value.  Contracts of one surface that share
+// (e^{Re Z} and Im Z without u x), node_finish adds one strike's phase and
+// forms the value.  Contracts of one surface that share
 // an expiry and a rate share node_cf's values at every panel they both
 // bisect (the run cache of quadrature.cuh).
 #pragma once
@@ -389,23 +389,30 @@ __device__ __forceinline__ double node_u(double omt, double tn, double itt) {
 }
 
 // The strike-free part of a node (heston.rs:221-227 with the merged-exponent
-// integrand): W = e^{Re Z} / ((1 - t) t), or NaN where the reference's g(t) is
-// 0 whatever the strike (t <= 0, u < 1e-12); A = Im Z - (u x mod 2 pi); u.
+// integrand): E = e^{Re Z}, A = Im Z - (u x mod 2 pi), and the node's
+// u = (1 - t)/t and itt = 1/((1 - t) t) (node_geom computes the last two
+// alone, bit for bit).
 struct NodeCf {
-    double w, a, u;
+    double e, a, u, itt;
 };
 
-// u of a node alone, as node_cf computes it (bit for bit).
-__device__ __forceinline__ double node_u_of(double tn) {
+__device__ __forceinline__ void node_geom(double tn, double& u, double& itt) {
     const double omt = 1.0 - tn;
-    return node_u(omt, tn, rcp_nr(omt * tn));
+    itt = rcp_nr(omt * tn);
+    u = node_u(omt, tn, itt);
+}
+
+// u of a node alone (bit for bit node_geom's).
+__device__ __forceinline__ double node_u_of(double tn) {
+    double u, itt;
+    node_geom(tn, u, itt);
+    return u;
 }
 
 template <bool BATES>
 __device__ __forceinline__ NodeCf node_cf(const CfConsts& C, double tn) {
-    const double omt = 1.0 - tn;
-    const double itt = rcp_nr(omt * tn);  // 1 / ((1 - t) t)
-    const double u = node_u(omt, tn, itt);    // (1 - t) / t
+    double u, itt;  // (1 - t) / t and 1 / ((1 - t) t)
+    node_geom(tn, u, itt);
     const double u2 = u * u;
     // xi = (xr, xi_) ; z = xi^2 + sigma^2 phi(phi+i)
     const double xr = C.xr, xi_ = -C.rs * u;
@@ -468,26 +475,45 @@ __device__ __forceinline__ NodeCf node_cf(const CfConsts& C, double tn) {
         zre += fma(je, jc, C.jre0);
         zim += fma(je, js, -C.ltc * u);
     }
-    const bool live = (tn > 0.0) && (u >= 1e-12);
-    return NodeCf{live ? __dmul_rn(exp(zre), itt) : __longlong_as_double(0x7ff8000000000000ll), zim, u};
+    return NodeCf{exp(zre), zim, u, itt};
 }
 
 // One strike's node value from the strike-free part: Im(e^Z) / u / t^2 =
-// e^{Re Z} sin(Im Z) / ((1 - t) t) = sin(A + phase) W, non-finite -> 0.
-// The phase of e^{iux} (heston.rs:107): u x rounded as the reference rounds
-// it, reduced modulo 2 pi without loss (Cody and Waite's argument reduction,
-// 2 pi split into two doubles and the products taken exactly by FMA:
-// |u x - n 2 pi| < 4 makes the first step exact), so that adding the CF's own
-// phase costs an ulp of a number below 4 however large u x is.  The
-// reference adds the two phases exactly too, through the complex product
-// e^{iux} CF (an unreduced sum would lose ulp(u x), 1e-9 at u x = 1e7, on
-// short-dated deep-wing contracts).
-__device__ __forceinline__ double node_finish(double x, const NodeCf& n) {
-    const double ux = __dmul_rn(n.u, x);
+// e^{Re Z} sin(Im Z) / ((1 - t) t) = sin(A + phase) W with W = E itt; 0
+// where the reference's g(t) is 0 (t <= 0, u < 1e-12) or the value is not
+// finite.  The phase of e^{iux} (heston.rs:107): u x rounded as the
+// reference rounds it, reduced modulo 2 pi without loss (Cody and Waite's
+// argument reduction, 2 pi split into two doubles and the products taken
+// exactly by FMA: |u x - n 2 pi| < 4 makes the first step exact), so that
+// adding the CF's own phase costs an ulp of a number below 4 however large
+// u x is.  The reference adds the two phases exactly too, through the
+// complex product e^{iux} CF (an unreduced sum would lose ulp(u x), 1e-9 at
+// u x = 1e7, on short-dated deep-wing contracts).
+// LIVE_IN_W: w already carries the liveness (NaN where the node is not live,
+// see node_w_live), as the run cache stores it; the value is then 0 exactly
+// where the explicit test gives 0.
+template <bool LIVE_IN_W = false>
+__device__ __forceinline__ double node_finish_w(double x, double tn, double w, double a, double u) {
+    const double ux = __dmul_rn(u, x);
     const double nq = rint(ux * 0.15915494309189535);  // 1 / (2 pi)
     const double uxr = fma(-nq, 2.4492935982947064e-16, fma(-nq, 6.283185307179586, ux));
-    const double v = __dmul_rn(sin(__dadd_rn(n.a, uxr)), n.w);
-    return isfinite(v) ? v : 0.0;
+    const double v = __dmul_rn(sin(__dadd_rn(a, uxr)), w);
+    const bool ok = (LIVE_IN_W || ((tn > 0.0) && (u >= 1e-12))) && isfinite(v);
+    return ok ? v : 0.0;
 }
+
+// W with the node's liveness folded in: NaN where the reference's g(t) is 0
+// whatever the strike (t <= 0, u < 1e-12).
+__device__ __forceinline__ double node_w_live(double tn, const NodeCf& n) {
+    return ((tn > 0.0) && (n.u >= 1e-12)) ? __dmul_rn(n.e, n.itt) : __longlong_as_double(0x7ff8000000000000ll);
+}
+
+__device__ __forceinline__ double node_w(const NodeCf& n) { return __dmul_rn(n.e, n.itt); }
+
+__device__ __forceinline__ double node_finish(double x, double tn, const NodeCf& n) {
+    return node_finish_w(x, tn, node_w(n), n.a, n.u);
+}
+
+
 
 }  // namespace ope

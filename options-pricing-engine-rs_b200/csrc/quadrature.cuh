@@ -129,8 +129,8 @@ __device__ __forceinline__ void gk_sums(double f, const LaneRule& R, double& Kl,
 // whose next panel is in the tree skips node_cf (the CF, its square root,
 // logarithm and exponentials) and pays only node_finish (its own phase and
 // one sin).  The tree lives in global memory (per warp: cap entries of 15
-// nodes x {w, a, u}); when it is full, further panels are evaluated
-// uncached.  The cached values are the ones node_cf returns (u is
+// nodes x {W, A}); when it is full, further panels are evaluated
+// uncached.  The cached values are the ones node_cf's result gives (u is
 // recomputed from the node, bit for bit), so a contract's price is
 // bit-identical with and without the cache.  An entry's w and a are one
 // 128-byte line each (15 nodes and a zero pad, written whole so that L2
@@ -139,8 +139,8 @@ constexpr uint16_t kNoEntry = 0xffff;
 constexpr uint32_t kNoChildren = 0xffffffffu;
 
 struct RunCacheWarp {
-    double* w;          // [cap][16]
-    double* a;          // [cap][16]
+    double* w;          // [cap][16]: W = e^{Re Z} / ((1 - t) t), NaN at nodes that are not live
+    double* a;          // [cap][16]: Im Z without the phase
     uint32_t* child;    // [cap]: children's entries, left | right << 16 (kNoChildren: none yet)
     uint16_t* slot;     // shared, [kMaxPanels]: entry of each live panel of the running integral
     int cap;            // entries (<= 65535)
@@ -153,10 +153,16 @@ struct RunCacheWarp {
 // its spills) out of the hit path.
 // (Internal linkage, so that ptxas allocates its registers within the
 // calling kernel's budget.)
+// It returns the cached form: W with the liveness folded in (node_w_live),
+// A and u.
 namespace {
+struct NodeW {
+    double w, a, u;
+};
 template <bool BATES>
-__device__ __noinline__ NodeCf node_cf_call(const CfConsts& C, double tn) {
-    return node_cf<BATES>(C, tn);
+__device__ __noinline__ NodeW node_cf_call(const CfConsts& C, double tn) {
+    const NodeCf n = node_cf<BATES>(C, tn);
+    return NodeW{node_w_live(tn, n), n.a, n.u};
 }
 }  // namespace
 
@@ -226,26 +232,39 @@ __device__ __forceinline__ double gk_integrate_warp(const CfConsts& C, double to
     }
     while (true) {
         const double c = 0.5 * (pa + pb), h = 0.5 * (pb - pa);
-        NodeCf nc{0.0, 0.0, 0.0};
+        const double tn = __dadd_rn(c, __dmul_rn(h, R.x));
+        // the node's strike-free part: W, A, u (from the tree on a hit)
+        double nw = 0.0, na = 0.0, nu = 0.0;
         if (CACHED && hit) {
             if (active) {
                 const size_t i = (size_t)(R.half ? er_ : el_) * 16 + (lane & 15);
-                nc = NodeCf{__ldcg(rc->w + i), __ldcg(rc->a + i), node_u_of(__dadd_rn(c, __dmul_rn(h, R.x)))};
+                nw = __ldcg(rc->w + i);
+                na = __ldcg(rc->a + i);
+                nu = node_u_of(tn);
             }
         } else {
             if (active) {
-                const double tn = __dadd_rn(c, __dmul_rn(h, R.x));
-                nc = CACHED ? node_cf_call<BATES>(C, tn) : node_cf<BATES>(C, tn);
+                if (CACHED) {
+                    const NodeW nc = node_cf_call<BATES>(C, tn);
+                    nw = nc.w;
+                    na = nc.a;
+                    nu = nc.u;
+                } else {
+                    const NodeCf nc = node_cf<BATES>(C, tn);
+                    nw = node_w(nc);
+                    na = nc.a;
+                    nu = nc.u;
+                }
             }
             // the half-warps that evaluated a child write its entry, the
             // pad lane (15 or 31) the 16th element
             if (CACHED && put && (active || (!R.node && (len > 0 || R.half == 0)))) {
                 const size_t i = (size_t)(R.half ? er_ : el_) * 16 + (lane & 15);
-                __stcg(rc->w + i, active ? nc.w : 0.0);
-                __stcg(rc->a + i, active ? nc.a : 0.0);
+                __stcg(rc->w + i, nw);
+                __stcg(rc->a + i, na);
             }
         }
-        const double f = active ? node_finish(C.x, nc) : 0.0;
+        const double f = active ? node_finish_w<CACHED>(C.x, tn, nw, na, nu) : 0.0;
         double Kl, Gl, Kr, Gr;
         gk_sums(f, R, Kl, Gl, Kr, Gr);
         if (len == 0) {
