@@ -130,7 +130,8 @@ uint64_t ope_workspace_bytes(void);
 /* No reference counterpart.  Reads and clears the device check word of a
  * bounds-checked build (make CHECKED=1, lib/checked/): each set bit is a
  * kernel invariant that failed and was contained (1 panel index, 2 panel
- * count, 4 surface index, 8 panel-list slot, 16 stored panel count).
+ * count, 4 surface index, 8 panel-list slot, 16 stored panel count, 32
+ * run-cache entry).
  * *out_checked_build: 1 for that build; the ordinary build reports 0 and a
  * zero word. */
 int ope_check_word(uint32_t* out_word, int32_t* out_checked_build);

@@ -19,6 +19,7 @@ enum : unsigned {
     CHK_SURFACE = 4u,      // parameter-set index outside [0, n_surf)
     CHK_SLOT = 8u,         // panel-list slot outside [0, n_slots)
     CHK_PANEL_LEN = 16u,   // stored bisection count outside [0, kMaxPanels)
+    CHK_RUN_ENTRY = 32u,   // run-cache entry outside the run's allocated entries
 };
 
 #if OPE_CHECKED

@@ -365,12 +365,18 @@ __device__ __forceinline__ double gk_integrate_warp(const CfConsts& C, double to
             sw_ = rc->slot[w];
             hit = put = false;
             el_ = er_ = kNoEntry;
+            if (sw_ != kNoEntry && !ope_check(sw_ < rc->n_alloc, CHK_RUN_ENTRY)) sw_ = kNoEntry;
             if (sw_ != kNoEntry) {
                 const uint32_t ch = rc->child[sw_];
                 if (ch != kNoChildren) {
                     hit = true;
                     el_ = (int)(ch & 0xffffu);
                     er_ = (int)(ch >> 16);
+                    if (!ope_check(el_ < rc->n_alloc && er_ < rc->n_alloc, CHK_RUN_ENTRY)) {
+                        hit = false;  // evaluate uncached
+                        el_ = er_ = kNoEntry;
+                        sw_ = kNoEntry;
+                    }
                 } else if (rc->n_alloc + 2 <= rc->cap) {
                     put = true;
                     el_ = rc->n_alloc;

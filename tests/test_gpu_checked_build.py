@@ -1,7 +1,7 @@
 """GPU: the bounds-checked build (lib/checked/, make CHECKED=1) runs the
-pricing, gradient, Greeks and calibration paths with its device invariant
-checks on -- panel-list indices and counts, surface indices, panel-list
-slots -- and must finish with a zero check word and the same results as the
+pricing (per contract and the run kernel), gradient, Greeks and calibration
+paths with its device invariant checks on -- panel-list indices and counts,
+surface indices, panel-list slots, run-cache entries -- and must finish with a zero check word and the same results as the
 ordinary build.  (A stand-in for a memory checker, which is not available
 on this pool.)"""
 import ctypes
@@ -47,6 +47,22 @@ def test_checked_build_runs_clean(ope, oracle):
     _ok(L, L.ope_batch_price_ex(1, w.contracts.ctypes.data, 256, w.params[0].ctypes.data, one.ctypes.data,
                                 ctypes.byref(o)))
     assert np.max(np.abs(one - ref[:256])) <= 1e-12 * S
+
+    # the run kernel (grid surfaces, 8 contracts per unit: the run cache's
+    # entries and child links checked) -- bit-identical to the ordinary build
+    g = W.c2(n_surf=120, seed=32)
+    E = (ope._lib.TuneEntry * ope._lib.TUNE_CLASSES)()
+    for e in E:
+        e.shape.warps_per_block, e.shape.occupancy, e.shape.per_unit = 4, 1.0, 8
+    _ok(L, L.ope_set_tune_table(0, E))
+    gpx = np.zeros(g.n)
+    _ok(L, L.ope_price_surfaces(0, g.contracts.ctypes.data, g.n, g.surf_offsets.ctypes.data, g.n_surf,
+                                g.params.ctypes.data, gpx.ctypes.data, ctypes.byref(o)))
+    pu = ctypes.c_int32()
+    _ok(L, L.ope_last_per_unit(ctypes.byref(pu)))
+    assert pu.value == 8
+    gref = ope.price_surfaces(ope.MODEL_HESTON, g.contracts, g.surf_offsets, g.params, tol=1e-10)
+    assert np.array_equal(gpx.view(np.int64), gref.view(np.int64))
 
     # reverse-mode gradient (panel lists stored by the pricing kernel, read by the backward pass)
     n = 1024
