@@ -209,3 +209,49 @@ def test_workspace_limit_drops_the_run_cache_not_the_call(ope, per_unit):
     finally:
         ope.set_workspace_limit(0)
     assert np.array_equal(got.view(np.int64), ref.view(np.int64))
+
+
+def _wide_grid(rng, n_surf, bates):
+    """Grid surfaces (expiry-major) over the wide ranges of the fuzz test:
+    vol-of-vol up to 3, correlation up to +-0.99, mean reversion 0.05 to 20,
+    expiries from one day to ten years, strikes deep in and out of the money,
+    jump intensities up to 5."""
+    parts, off, pars = [], [0], []
+    for _ in range(n_surf):
+        r, q = rng.uniform(-0.01, 0.08), rng.uniform(0.0, 0.05)
+        ts = np.sort(np.exp(rng.uniform(np.log(1 / 365), np.log(10.0), rng.integers(2, 8))))
+        ms = np.sort(rng.uniform(-2.0, 1.2, rng.integers(4, 24)))
+        T, M = np.meshgrid(ts, ms, indexing="ij")
+        c = np.zeros(T.size, W.CONTRACT_DTYPE)
+        c["spot"], c["expiry"] = S, T.ravel()
+        c["strike"] = S * np.exp((r - q) * T.ravel() + M.ravel() * np.sqrt(np.minimum(T.ravel(), 1.0)))
+        c["rate"], c["div_yield"], c["vol"] = r, q, 0.2
+        c["opt_type"] = rng.integers(0, 2, T.size)
+        parts.append(c)
+        off.append(off[-1] + c.size)
+        p = [rng.uniform(0.005, 0.6), np.exp(rng.uniform(np.log(0.05), np.log(20.0))), rng.uniform(0.005, 0.6),
+             rng.uniform(0.05, 3.0), rng.uniform(-0.99, 0.99)]
+        if bates:
+            p += [rng.uniform(0.0, 5.0), rng.uniform(-0.5, 0.3), rng.uniform(0.02, 0.6)]
+        pars.append(p)
+    return np.concatenate(parts), np.array(off, np.int64), np.array(pars)
+
+
+@pytest.mark.parametrize("bates", [False, True])
+def test_wide_range_grids_bitwise_in_the_run_kernel(ope, oracle, per_unit, bates):
+    """Wide-range grids: the run kernel (8 contracts per unit) gives the
+    per-contract kernel's bits, and both the oracle's prices to 1e-9 S on a
+    sample (non-finite where the reference's formula is)."""
+    rng = np.random.default_rng(4040 + bates)
+    con, off, params = _wide_grid(rng, 700, bates)
+    model = ope.MODEL_BATES if bates else ope.MODEL_HESTON
+    out, used = _all_modes(ope, per_unit, model, con, off, params, modes=(1, 8))
+    assert used[8] == 8
+    a, b = out[1], out[8]
+    assert np.array_equal(a.view(np.int64), b.view(np.int64))
+    pick = np.sort(rng.choice(con.size, 800, replace=False))
+    sidx = np.repeat(np.arange(off.size - 1), np.diff(off)).astype(np.int32)
+    ref = oracle.batch_price(con[pick], params, bates, 1e-10, surf_idx=sidx[pick])
+    fin = np.isfinite(ref)
+    assert np.array_equal(np.isfinite(b[pick]), fin)
+    assert float(np.max(np.abs(b[pick][fin] - ref[fin]))) <= PRICE_TOL
