@@ -64,6 +64,7 @@ int ensure_device() {
     // rather than freed on the wrong device).
     c.ws = nullptr;
     c.ws_bytes = 0;
+    c.last_probe = nullptr;
     OPE_CHECK(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
     c.device = cur;
     c.sm_count = sms;
@@ -429,6 +430,12 @@ int ope_set_workspace_limit(uint64_t bytes) {
     if (bytes && c.ws && c.ws_bytes > bytes) {  // give back a workspace above the new cap
         // stream-ordered after the workspace's last use (its event), on this
         // thread's own stream (created with the workspace's device)
+        if (c.last_probe) {  // the run probe's word lives in the workspace: keep what it said
+            int32_t pu = 1;
+            OPE_TRY(ope_last_per_unit(&pu));
+            c.last_per_unit = pu;
+            c.last_probe = nullptr;
+        }
         if (c.ws_recorded) OPE_CHECK(cudaStreamWaitEvent(c.stream, c.ws_event, 0));
         OPE_CHECK(cudaFreeAsync(c.ws, c.stream));
         c.ws = nullptr;

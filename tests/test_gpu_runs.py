@@ -201,9 +201,11 @@ def test_workspace_limit_drops_the_run_cache_not_the_call(ope, per_unit):
     con, off, params = _grid(900, seed=26)
     per_unit(ope.MODEL_HESTON, 0)
     ref = _prices(ope, ope.MODEL_HESTON, con, off, params)
-    assert ope.last_per_unit() >= 4
+    chosen = ope.last_per_unit()
+    assert chosen >= 4
     try:
-        ope.set_workspace_limit(96 << 20)
+        ope.set_workspace_limit(96 << 20)  # releases the workspace the probe's word was in
+        assert ope.last_per_unit() == chosen
         got = _prices(ope, ope.MODEL_HESTON, con, off, params)
         assert ope.last_per_unit() == 1
     finally:
